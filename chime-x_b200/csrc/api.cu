@@ -1,0 +1,258 @@
+// api.cu -- C ABI of libchimex: plans and the plain-path entry points.
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "chimex_internal.h"
+
+namespace chx {
+
+static thread_local char g_err[512] = "";
+
+int fail(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(e == cudaErrorMemoryAllocation ? CHX_E_NOMEM : CHX_E_CUDA, "%s: %s (%s)",
+                what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+void clear_error() { g_err[0] = 0; }
+
+}  // namespace chx
+
+using namespace chx;
+
+extern "C" {
+
+const char *chx_version(void) { return "chimex-b200 0.1"; }
+
+const char *chx_last_error(void) { return g_err; }
+
+int chx_plan_create(chx_plan **plan, int E, int F, int T, int TA, int ut, int kernel_batch,
+                    int device) {
+    clear_error();
+    if (!plan) return fail(CHX_E_INVALID, "plan pointer is NULL");
+    *plan = nullptr;
+    if (E < 32 || E % 32 != 0)
+        return fail(CHX_E_INVALID, "num_elements=%d must be a positive multiple of 32", E);
+    if (E > 65536) return fail(CHX_E_UNSUPPORTED, "num_elements=%d exceeds 65536", E);
+    if (F < 1) return fail(CHX_E_INVALID, "num_frequencies=%d must be >= 1", F);
+    if (T < 1 || T > 16777215)
+        return fail(CHX_E_INVALID, "num_timesamples=%d outside [1, 16777215]", T);
+    if (TA < 1) return fail(CHX_E_INVALID, "time_accum=%d must be >= 1", TA);
+    if (ut != 0 && ut != 1)
+        return fail(CHX_E_INVALID, "upper_triangle_convention=%d not in {0,1}", ut);
+    if (kernel_batch != 0 && kernel_batch != 1)
+        return fail(CHX_E_INVALID, "kernel_batch=%d not in {0,1}", kernel_batch);
+    int ndev = 0;
+    CHX_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev)
+        return fail(CHX_E_INVALID, "device=%d outside [0,%d)", device, ndev);
+    DeviceGuard g(device);
+    if (!g.ok) return fail(CHX_E_CUDA, "cudaSetDevice(%d) failed", device);
+    chx_plan *p = new (std::nothrow) chx_plan();
+    if (!p) return fail(CHX_E_NOMEM, "host allocation failed");
+    p->E = E;
+    p->F = F;
+    p->T = T;
+    p->TA = TA;
+    p->ut = ut;
+    p->kernel_batch = kernel_batch;
+    p->device = device;
+    p->NB1 = E / 32;
+    p->NB = num_blocks_of(E);
+    p->algo = CHX_ALGO_AUTO;
+    p->tsplit = 0;
+    p->tile = 0;
+    p->d_err = nullptr;
+    cudaError_t e = cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        if (p->d_err) cudaFree(p->d_err);
+        delete p;
+        return cuda_fail(e, "plan device state");
+    }
+    *plan = p;
+    return CHX_OK;
+}
+
+int chx_plan_destroy(chx_plan *p) {
+    clear_error();
+    if (!p) return CHX_OK;
+    DeviceGuard g(p->device);
+    if (p->d_err) cudaFree(p->d_err);
+    delete p;
+    return CHX_OK;
+}
+
+int chx_plan_set_option(chx_plan *p, int option, int64_t value) {
+    clear_error();
+    if (!p) return fail(CHX_E_INVALID, "plan is NULL");
+    switch (option) {
+    case CHX_OPT_ALGO:
+        if (value < CHX_ALGO_AUTO || value > CHX_ALGO_TC)
+            return fail(CHX_E_INVALID, "unknown algorithm %lld", (long long)value);
+        if (value == CHX_ALGO_TC && !tc_supported(p->E, p->T))
+            return fail(CHX_E_UNSUPPORTED, "tensor-core path does not take E=%d T=%d", p->E, p->T);
+        p->algo = (int)value;
+        return CHX_OK;
+    case CHX_OPT_TSPLIT:
+        if (value < 0 || value > 4096) return fail(CHX_E_INVALID, "tsplit %lld", (long long)value);
+        p->tsplit = (int)value;
+        return CHX_OK;
+    case CHX_OPT_TILE:
+        if (value < 0 || value > 16) return fail(CHX_E_INVALID, "tile %lld", (long long)value);
+        p->tile = (int)value;
+        return CHX_OK;
+    default:
+        return fail(CHX_E_INVALID, "unknown option %d", option);
+    }
+}
+
+int64_t chx_plan_block_words(const chx_plan *p) { return p ? (int64_t)p->F * p->NB * 2048 : -1; }
+int64_t chx_plan_input_bytes(const chx_plan *p) {
+    return p ? (int64_t)p->T * p->F * p->E : -1;
+}
+int64_t chx_plan_sum_words(const chx_plan *p) { return p ? (int64_t)p->F * p->E * 2 : -1; }
+int64_t chx_plan_triangle_words(const chx_plan *p) {
+    return p ? (int64_t)p->F * p->E * (p->E + 1) : -1;
+}
+
+// Sample-range splits for a plain-path launch of `units` independent output
+// tiles: enough CTAs to fill the SMs several times, never below 1.
+static int auto_splits(int64_t units, int T, int sm_count, int min_chunk) {
+    int64_t want = (int64_t)sm_count * 4;
+    int s = 1;
+    while (units * s < want && T / (2 * s) >= min_chunk) s *= 2;
+    return s;
+}
+
+int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void *stream,
+                  int accumulate) {
+    clear_error();
+    if (!p || !d_packed || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
+    DeviceGuard g(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool use_tc =
+        (p->algo == CHX_ALGO_TC) || (p->algo == CHX_ALGO_AUTO && tc_supported(p->E, p->T));
+    if (use_tc) {
+        TcArgs a;
+        a.packed = d_packed;
+        a.in_stride = (int64_t)p->F * p->E;
+        a.chan_stride = p->E;
+        a.blocks = d_blocks;
+        a.out_chan_stride = p->NB * 2048;
+        a.E = p->E;
+        a.F = p->F;
+        a.T = p->T;
+        a.map = MAP_EXACT;
+        a.ut = p->ut;
+        a.splits = p->tsplit;  // 0 = let the launcher decide
+        a.mode = accumulate ? 1 : 0;
+        a.err = p->d_err;
+        CHX_CUDA(launch_correlate_tc(a, p->sm_count, st));
+        return CHX_OK;
+    }
+    const int splits =
+        p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);
+    int mode;
+    if (splits > 1) {
+        if (!accumulate)
+            CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)chx_plan_block_words(p) * 4, st));
+        mode = 2;
+    } else {
+        mode = accumulate ? 1 : 0;
+    }
+    CHX_CUDA(launch_correlate_simt(d_packed, d_blocks, p->E, p->F, p->T, MAP_EXACT, p->ut,
+                                   mode, splits, st));
+    return CHX_OK;
+}
+
+int chx_offset_accumulate(chx_plan *p, const uint8_t *d_packed, uint32_t *d_sums,
+                          void *stream, int accumulate) {
+    clear_error();
+    if (!p || !d_packed || !d_sums) return fail(CHX_E_INVALID, "NULL argument");
+    DeviceGuard g(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!accumulate)
+        CHX_CUDA(cudaMemsetAsync(d_sums, 0, (size_t)chx_plan_sum_words(p) * 4, st));
+    CHX_CUDA(launch_offset_accumulate(d_packed, d_sums, p->E, p->F, p->T, st));
+    return CHX_OK;
+}
+
+int chx_preseed(chx_plan *p, const uint32_t *d_sums, int32_t *d_blocks, void *stream) {
+    clear_error();
+    if (!p || !d_sums || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
+    DeviceGuard g(p->device);
+    CHX_CUDA(launch_preseed(d_sums, d_blocks, p->E, p->F, p->T, p->kernel_batch, p->ut,
+                            (cudaStream_t)stream));
+    return CHX_OK;
+}
+
+int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void *stream) {
+    clear_error();
+    if (!p || !d_packed || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
+    // The reference kernels' own domain (main_wrapper.c:564-569,
+    // pairwise_correlator_UT.cl:82, help text main_wrapper.c:57).
+    if (p->T % p->TA != 0)
+        return fail(CHX_E_INVALID, "T=%d is not a multiple of time_accum=%d", p->T, p->TA);
+    if (p->TA % 8 != 0)
+        return fail(CHX_E_INVALID, "time_accum=%d is not a multiple of 8", p->TA);
+    if (p->T % 32 != 0) return fail(CHX_E_INVALID, "T=%d is not a multiple of 32", p->T);
+    if (p->kernel_batch == CHX_KERNEL_CONFERENCE && p->TA > 291)
+        return fail(CHX_E_INVALID, "time_accum=%d > 291 overflows the conference kernel", p->TA);
+    if (p->kernel_batch == CHX_KERNEL_PACKED && p->TA > 2272)
+        return fail(CHX_E_INVALID, "time_accum=%d > 2272 overflows the packed kernel", p->TA);
+    if (p->kernel_batch == CHX_KERNEL_PACKED && p->F != 1)
+        return fail(CHX_E_UNSUPPORTED,
+                    "the packed reference kernel has no channel index: F must be 1 (F=%d)", p->F);
+    DeviceGuard g(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int map = p->kernel_batch == CHX_KERNEL_PACKED ? MAP_PACKED : MAP_CONF;
+    const int splits =
+        p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);
+    CHX_CUDA(launch_correlate_simt(d_packed, d_blocks, p->E, p->F, p->T, map, p->ut,
+                                   splits > 1 ? 2 : 1, splits, st));
+    return CHX_OK;
+}
+
+int chx_blocks_to_triangle(chx_plan *p, const int32_t *d_blocks, int32_t *d_tri, void *stream) {
+    clear_error();
+    if (!p || !d_blocks || !d_tri) return fail(CHX_E_INVALID, "NULL argument");
+    DeviceGuard g(p->device);
+    CHX_CUDA(launch_blocks_to_triangle(d_blocks, d_tri, p->E, p->F, (cudaStream_t)stream));
+    return CHX_OK;
+}
+
+int chx_blocks_to_full(chx_plan *p, const int32_t *d_blocks, int32_t *d_full, void *stream) {
+    clear_error();
+    if (!p || !d_blocks || !d_full) return fail(CHX_E_INVALID, "NULL argument");
+    DeviceGuard g(p->device);
+    CHX_CUDA(launch_blocks_to_full(d_blocks, d_full, p->E, p->F, (cudaStream_t)stream));
+    return CHX_OK;
+}
+
+int chx_plan_check(chx_plan *p, void *stream) {
+    clear_error();
+    if (!p) return fail(CHX_E_INVALID, "plan is NULL");
+    DeviceGuard g(p->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int h = 0;
+    CHX_CUDA(cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CHX_CUDA(cudaStreamSynchronize(st));
+    if (h != 0) {
+        CHX_CUDA(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+        CHX_CUDA(cudaStreamSynchronize(st));
+        return fail(CHX_E_TIMEOUT, "a bounded device wait gave up (code 0x%x)", h);
+    }
+    return CHX_OK;
+}
+
+}  // extern "C"

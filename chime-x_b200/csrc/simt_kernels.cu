@@ -1,0 +1,323 @@
+// simt_kernels.cu -- CUDA-core kernels of libchimex:
+//   * correlate_simt: dp4a correlator over 32x32 blocks (baseline path and the
+//     fallback for shapes the tensor-core kernel does not take; also used by
+//     chx_corr_compat with the offset-domain value maps),
+//   * offset_accumulate: offsetAccumulateElements (offset_accumulator.cl:7-49),
+//   * preseed: the four preseed variants (preseed_multifreq*_UT.cl),
+//   * block -> triangle / full-matrix reorganisation (gpu_data_reorg.c:36-124).
+#include "chimex_internal.h"
+
+namespace chx {
+
+namespace {
+
+// (by, bx) of block b in the row-major upper-triangle enumeration of
+// main_wrapper.c:529-540.
+__device__ __forceinline__ void decode_block(int b, int nb1, int &by, int &bx) {
+    int r = b, y = 0;
+    while (r >= nb1 - y) {
+        r -= nb1 - y;
+        y++;
+    }
+    by = y;
+    bx = y + r;
+}
+
+// Operand bytes of one packed sample under a value map (see chimex_internal.h).
+struct Ops {
+    int a0, a1, b0, b1, b2, b3;
+};
+
+template <int MAP>
+__device__ __forceinline__ Ops map_byte(uint32_t p) {
+    const int hi = (p >> 4) & 15, lo = p & 15;
+    Ops o;
+    if (MAP == MAP_EXACT) {
+        o.a0 = hi - 8; o.a1 = lo - 8;
+        o.b0 = hi - 8; o.b1 = lo - 8; o.b2 = 8 - lo; o.b3 = hi - 8;
+    } else if (MAP == MAP_CONF) {
+        o.a0 = hi; o.a1 = lo;
+        o.b0 = hi; o.b1 = lo; o.b2 = -lo; o.b3 = hi;
+    } else {
+        o.a0 = hi; o.a1 = 15 - lo;
+        o.b0 = hi; o.b1 = -lo; o.b2 = -lo; o.b3 = -hi;
+    }
+    return o;
+}
+
+__device__ __forceinline__ uint32_t put_byte(uint32_t w, int v, int j) {
+    return w | ((uint32_t)(v & 0xFF) << (8 * j));
+}
+
+// One CTA = one 32x32 output block of one channel over one sample range.
+// Each of the 256 threads owns a 2x2 group of cells.  Samples are staged 32
+// at a time: packed bytes -> shared memory -> int8x4 words per element
+// ([component][word][element], conflict-free for the compute loop).
+template <int MAP>
+__global__ void __launch_bounds__(256)
+correlate_simt_kernel(const uint8_t *__restrict__ packed, int32_t *__restrict__ blocks,
+                      int E, int F, int T, int nb1, int64_t nb, int ut, int mode,
+                      int tchunk) {
+    __shared__ uint32_t py[32][8];  // [sample][element/4] packed bytes
+    __shared__ uint32_t px[32][8];
+    __shared__ int32_t A[2][8][32];  // [a0|a1][sample/4][element]
+    __shared__ int32_t B[4][8][32];  // [b0..b3][sample/4][element]
+
+    const int b = blockIdx.x, f = blockIdx.y;
+    int by, bx;
+    decode_block(b, nb1, by, bx);
+    const int t_begin = blockIdx.z * tchunk;
+    const int t_end = min(T, t_begin + tchunk);
+    const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+    const int64_t row = (int64_t)F * E;
+    const uint8_t *base = packed + (int64_t)f * E;
+
+    int re[2][2] = {{0, 0}, {0, 0}}, im[2][2] = {{0, 0}, {0, 0}};
+
+    for (int t0 = t_begin; t0 < t_end; t0 += 32) {
+        {
+            const int r = tid >> 3, c = tid & 7;
+            const int t = t0 + r;
+            uint32_t vy = 0, vx = 0;
+            if (t < t_end) {
+                vy = *reinterpret_cast<const uint32_t *>(base + t * row + by * 32 + c * 4);
+                vx = *reinterpret_cast<const uint32_t *>(base + t * row + bx * 32 + c * 4);
+            }
+            py[r][c] = vy;
+            px[r][c] = vx;
+        }
+        __syncthreads();
+        {
+            const int e = tid & 31, w = tid >> 5;
+            uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int s = 4 * w + j;
+                if (t0 + s < t_end) {
+                    const uint32_t pyb = (py[s][e >> 2] >> (8 * (e & 3))) & 0xFF;
+                    const uint32_t pxb = (px[s][e >> 2] >> (8 * (e & 3))) & 0xFF;
+                    const Ops oy = map_byte<MAP>(pyb), ox = map_byte<MAP>(pxb);
+                    a0 = put_byte(a0, oy.a0, j);
+                    a1 = put_byte(a1, oy.a1, j);
+                    b0 = put_byte(b0, ox.b0, j);
+                    b1 = put_byte(b1, ox.b1, j);
+                    b2 = put_byte(b2, ox.b2, j);
+                    b3 = put_byte(b3, ox.b3, j);
+                }
+            }
+            A[0][w][e] = (int32_t)a0;
+            A[1][w][e] = (int32_t)a1;
+            B[0][w][e] = (int32_t)b0;
+            B[1][w][e] = (int32_t)b1;
+            B[2][w][e] = (int32_t)b2;
+            B[3][w][e] = (int32_t)b3;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int w = 0; w < 8; w++) {
+            int ya0[2], ya1[2], xb0[2], xb1[2], xb2[2], xb3[2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                ya0[i] = A[0][w][2 * ty + i];
+                ya1[i] = A[1][w][2 * ty + i];
+                xb0[i] = B[0][w][2 * tx + i];
+                xb1[i] = B[1][w][2 * tx + i];
+                xb2[i] = B[2][w][2 * tx + i];
+                xb3[i] = B[3][w][2 * tx + i];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    re[i][j] = __dp4a(ya0[i], xb0[j], re[i][j]);
+                    re[i][j] = __dp4a(ya1[i], xb1[j], re[i][j]);
+                    im[i][j] = __dp4a(ya0[i], xb2[j], im[i][j]);
+                    im[i][j] = __dp4a(ya1[i], xb3[j], im[i][j]);
+                }
+        }
+        __syncthreads();
+    }
+
+    int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int y = 2 * ty + i, x = 2 * tx + j;
+            const int vr = re[i][j];
+            const int vi = ut ? im[i][j] : (int)(0u - (uint32_t)im[i][j]);
+            int32_t *cell = blk + y * 64 + 2 * x;
+            if (mode == 0) {
+                *reinterpret_cast<int2 *>(cell) = make_int2(vr, vi);
+            } else if (mode == 1) {
+                int2 o = *reinterpret_cast<int2 *>(cell);
+                o.x = (int)((uint32_t)o.x + (uint32_t)vr);
+                o.y = (int)((uint32_t)o.y + (uint32_t)vi);
+                *reinterpret_cast<int2 *>(cell) = o;
+            } else {
+                atomicAdd(cell, vr);
+                atomicAdd(cell + 1, vi);
+            }
+        }
+}
+
+// offsetAccumulateElements: each thread owns 4 consecutive (f, e) bytes and a
+// sample range; nibbles are summed four lanes at a time in byte-wide SWAR
+// registers (15 * 16 < 256) and flushed to 32-bit sums every 16 samples.
+__global__ void __launch_bounds__(256)
+offset_accumulate_kernel(const uint8_t *__restrict__ packed, uint32_t *__restrict__ sums,
+                         int64_t nwords, int T, int tchunk) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nwords) return;
+    const int t_begin = blockIdx.y * tchunk;
+    const int t_end = min(T, t_begin + tchunk);
+    const uint32_t *p = reinterpret_cast<const uint32_t *>(packed);
+    uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = t_begin; t < t_end; t += 16) {
+        uint32_t lo4 = 0, hi4 = 0;
+        const int n = min(16, t_end - t);
+        for (int k = 0; k < n; k++) {
+            const uint32_t w = __ldg(p + (int64_t)(t + k) * nwords + i);
+            lo4 += w & 0x0F0F0F0Fu;
+            hi4 += (w >> 4) & 0x0F0F0F0Fu;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            s[2 * j] += (hi4 >> (8 * j)) & 0xFF;
+            s[2 * j + 1] += (lo4 >> (8 * j)) & 0xFF;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; j++) atomicAdd(sums + 8 * i + j, s[j]);
+}
+
+// preseed: writes (=) the offset correction of every cell of one block.
+// Formulas: preseed_multifreq_UT.cl:54-70 / preseed_multifreq.cl:54-70
+// (conference) and preseed_multifreq_highly_packed_correlator_method{_UT,}.cl
+// :54-70 (packed); x is the column element, y the row element.
+__global__ void __launch_bounds__(256)
+preseed_kernel(const uint32_t *__restrict__ sums, int32_t *__restrict__ blocks, int E,
+               int nb1, int64_t nb, uint32_t t128, int packed_variant, int ut) {
+    __shared__ uint32_t sx[64], sy[64];
+    const int b = blockIdx.x, f = blockIdx.y;
+    int by, bx;
+    decode_block(b, nb1, by, bx);
+    const int tid = threadIdx.x;
+    if (tid < 64) {
+        sx[tid] = sums[((int64_t)f * E + bx * 32) * 2 + tid];
+        sy[tid] = sums[((int64_t)f * E + by * 32) * 2 + tid];
+    }
+    __syncthreads();
+    int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int c = tid + 256 * k, yl = c >> 5, xl = c & 31;
+        const uint32_t xr = sx[2 * xl], xi = sx[2 * xl + 1];
+        const uint32_t yr = sy[2 * yl], yi = sy[2 * yl + 1];
+        uint32_t re, imv;
+        if (!packed_variant) {
+            re = t128 - 8u * (xr + xi + yr + yi);
+            imv = ut ? 8u * ((xi - xr) + (yr - yi)) : 8u * ((xr - xi) + (yi - yr));
+        } else {
+            re = t128 - 8u * xr + 7u * xi - 8u * (yr + yi);
+            imv = ut ? 8u * xi + 7u * xr + 8u * (yr - yi)
+                     : 0u - 8u * xi - 7u * xr - 8u * (yr - yi);
+        }
+        *reinterpret_cast<int2 *>(blk + c * 2) = make_int2((int)re, (int)imv);
+    }
+}
+
+// Block layout -> packed triangle (gpu_data_reorg.c:76-124).
+__global__ void __launch_bounds__(256)
+blocks_to_triangle_kernel(const int32_t *__restrict__ blocks, int32_t *__restrict__ tri,
+                          int E, int nb1, int64_t nb) {
+    const int b = blockIdx.x, f = blockIdx.y;
+    int by, bx;
+    decode_block(b, nb1, by, bx);
+    const int64_t ntri = (int64_t)E * (E + 1) / 2;
+    const int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int c = threadIdx.x + 256 * k, yl = c >> 5, xl = c & 31;
+        if (bx == by && xl < yl) continue;
+        const int64_t y = by * 32 + yl, x = bx * 32 + xl;
+        const int64_t a = f * ntri + y * E - (y - 1) * y / 2 + (x - y);
+        *reinterpret_cast<int2 *>(tri + 2 * a) = *reinterpret_cast<const int2 *>(blk + 2 * c);
+    }
+}
+
+// Block layout -> full Hermitian matrix (gpu_data_reorg.c:36-74).
+__global__ void __launch_bounds__(256)
+blocks_to_full_kernel(const int32_t *__restrict__ blocks, int32_t *__restrict__ full,
+                      int E, int nb1, int64_t nb) {
+    const int b = blockIdx.x, f = blockIdx.y;
+    int by, bx;
+    decode_block(b, nb1, by, bx);
+    const int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
+    int32_t *m = full + (int64_t)f * E * E * 2;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int c = threadIdx.x + 256 * k, yl = c >> 5, xl = c & 31;
+        const int64_t y = by * 32 + yl, x = bx * 32 + xl;
+        if (x < y) continue;
+        const int2 v = *reinterpret_cast<const int2 *>(blk + 2 * c);
+        *reinterpret_cast<int2 *>(m + (y * E + x) * 2) = v;
+        if (x > y)
+            *reinterpret_cast<int2 *>(m + (x * E + y) * 2) =
+                make_int2(v.x, (int)(0u - (uint32_t)v.y));
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_correlate_simt(const uint8_t *packed, int32_t *blocks, int E, int F,
+                                  int T, int map, int ut, int mode, int splits,
+                                  cudaStream_t st) {
+    const int nb1 = E / 32;
+    const int64_t nb = num_blocks_of(E);
+    if (splits < 1) splits = 1;
+    int tchunk = (T + splits - 1) / splits;
+    tchunk = (tchunk + 31) / 32 * 32;
+    splits = (T + tchunk - 1) / tchunk;
+    dim3 grid((unsigned)nb, (unsigned)F, (unsigned)splits);
+    if (map == MAP_EXACT)
+        correlate_simt_kernel<MAP_EXACT><<<grid, 256, 0, st>>>(packed, blocks, E, F, T, nb1, nb, ut, mode, tchunk);
+    else if (map == MAP_CONF)
+        correlate_simt_kernel<MAP_CONF><<<grid, 256, 0, st>>>(packed, blocks, E, F, T, nb1, nb, ut, mode, tchunk);
+    else
+        correlate_simt_kernel<MAP_PACKED><<<grid, 256, 0, st>>>(packed, blocks, E, F, T, nb1, nb, ut, mode, tchunk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_offset_accumulate(const uint8_t *packed, uint32_t *sums, int E, int F,
+                                     int T, cudaStream_t st) {
+    const int64_t nwords = (int64_t)F * E / 4;
+    const int tchunk = 512;
+    dim3 grid((unsigned)((nwords + 255) / 256), (unsigned)((T + tchunk - 1) / tchunk));
+    offset_accumulate_kernel<<<grid, 256, 0, st>>>(packed, sums, nwords, T, tchunk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preseed(const uint32_t *sums, int32_t *blocks, int E, int F, int T,
+                           int packed_variant, int ut, cudaStream_t st) {
+    dim3 grid((unsigned)num_blocks_of(E), (unsigned)F);
+    preseed_kernel<<<grid, 256, 0, st>>>(sums, blocks, E, E / 32, num_blocks_of(E),
+                                         (uint32_t)T * 128u, packed_variant, ut);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blocks_to_triangle(const int32_t *blocks, int32_t *tri, int E, int F,
+                                      cudaStream_t st) {
+    dim3 grid((unsigned)num_blocks_of(E), (unsigned)F);
+    blocks_to_triangle_kernel<<<grid, 256, 0, st>>>(blocks, tri, E, E / 32, num_blocks_of(E));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_blocks_to_full(const int32_t *blocks, int32_t *full, int E, int F,
+                                  cudaStream_t st) {
+    dim3 grid((unsigned)num_blocks_of(E), (unsigned)F);
+    blocks_to_full_kernel<<<grid, 256, 0, st>>>(blocks, full, E, E / 32, num_blocks_of(E));
+    return cudaGetLastError();
+}
+
+}  // namespace chx

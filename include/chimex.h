@@ -1,0 +1,221 @@
+/*
+ * chimex.h -- C ABI of libchimex, the B200 (sm_100a) CHIME X-engine.
+ *
+ * Drop-in replacement for the device side of CHIME-x's correlator_test: the
+ * reference builds three OpenCL kernels (corr, offsetAccumulateElements,
+ * preseed) with the problem size baked in as -D macros
+ * (main_wrapper.c:309-372) and launches them on an event-chained queue
+ * (main_wrapper.c:693-777).  Here the problem size lives in a plan, every
+ * kernel takes plain device pointers, and the fused chx_correlate replaces the
+ * whole accumulate -> preseed -> corr chain.
+ *
+ * Data contract (identical to the reference):
+ *   input   uint8 [T][F][E]: byte = (re+8)<<4 | (im+8), re, im in [-8, 7]
+ *           (four_bit_macros.h:8-9, input_generator.c:58,85)
+ *   output  int32 [F][NB][32][32][2] (re, im) with NB = (E/32)(E/32+1)/2
+ *           blocks enumerated row-major over the upper triangle
+ *           (main_wrapper.c:529-540), cell (y, x) = V[y][x] with y the row
+ *           element, x >= y's block column; diagonal blocks hold all 32x32
+ *           cells (pairwise_correlator_UT.cl:161, gpu_data_reorg.c:76-124).
+ *   V[y][x] = sum_t s_y conj(s_x) for upper_triangle_convention = 1
+ *           (cpu_corr_test.c:188-193); the imaginary part is negated for 0
+ *           (cpu_corr_test.c:91-96).
+ *
+ * Conventions: every function returns CHX_OK (0) or a negative CHX_E_* code
+ * and sets a thread-local message readable with chx_last_error().  Device
+ * pointers and streams are owned by the caller; the library owns its plans,
+ * their small device-side tables and any scratch a plan allocates at
+ * creation.  Work is enqueued asynchronously on the given stream (a
+ * cudaStream_t passed as void*; NULL = the legacy default stream).  A plan is
+ * thread-compatible: one thread at a time per plan.
+ */
+#ifndef CHIMEX_H
+#define CHIMEX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHX_OK 0
+#define CHX_E_INVALID (-1)     /* bad argument or shape */
+#define CHX_E_UNSUPPORTED (-2) /* valid, but outside what this build handles */
+#define CHX_E_CUDA (-3)        /* a CUDA runtime call failed */
+#define CHX_E_NOMEM (-4)       /* device or host allocation failed */
+#define CHX_E_TIMEOUT (-5)     /* a bounded device-side wait gave up */
+#define CHX_E_NOT_READY (-6)   /* asynchronous result not available yet */
+#define CHX_E_ADMISSION (-7)   /* streaming admission refused (HBM budget) */
+
+/* Kernel families of the reference (main_wrapper.c:282-305, -k flag). */
+#define CHX_KERNEL_CONFERENCE 0 /* pairwise_correlator*.cl + preseed_multifreq*.cl */
+#define CHX_KERNEL_PACKED 1     /* packed_correlator_overflow_protected_to_2272_iter*.cl */
+
+/* Algorithms for the fused plain path (chx_plan_set_option CHX_OPT_ALGO). */
+#define CHX_ALGO_AUTO 0 /* tensor-core path when the shape allows it */
+#define CHX_ALGO_SIMT 1 /* CUDA-core dp4a kernel (baseline / small shapes) */
+#define CHX_ALGO_TC 2   /* tcgen05 kind::i8 kernel */
+
+/* Plan options. */
+#define CHX_OPT_ALGO 1      /* one of CHX_ALGO_* */
+#define CHX_OPT_TSPLIT 2    /* number of sample-range splits (0 = auto) */
+#define CHX_OPT_TILE 3      /* tensor-core tile variant (0 = auto) */
+
+typedef struct chx_plan chx_plan;
+
+/* Library version, e.g. "chimex-b200 0.1". */
+const char *chx_version(void);
+
+/* Message describing the last failure on this thread ("" if none). */
+const char *chx_last_error(void);
+
+/* Creates a plan for E elements, F channels, T samples per call.
+ * Replaces the -D NUM_ELEMENTS/NUM_FREQUENCIES/NUM_BLOCKS/NUM_TIMESAMPLES/
+ * NUM_TIME_ACCUM build of main_wrapper.c:277-312.  Requires E % 32 == 0
+ * (32-element blocks, main_wrapper.c:277-278), F >= 1, 1 <= T <= 16777215
+ * (int32 exactness: |Re|, |Im| <= 128 T), upper_triangle_convention in
+ * {0, 1}, kernel_batch in {0, 1}.  time_accum only constrains the reference
+ * compatibility kernels (chx_corr_compat); the fused path is exact for any
+ * T and time_accum.  device = CUDA ordinal. */
+int chx_plan_create(chx_plan **plan, int num_elements, int num_frequencies,
+                    int num_timesamples, int time_accum,
+                    int upper_triangle_convention, int kernel_batch, int device);
+int chx_plan_destroy(chx_plan *plan);
+
+/* Sets an option (CHX_OPT_*) on a plan. */
+int chx_plan_set_option(chx_plan *plan, int option, int64_t value);
+
+/* Sizes in elements: output block buffer (F*NB*2048 int32), packed input
+ * (T*F*E bytes), offset sums (F*E*2 uint32), triangle (F*E*(E+1) int32). */
+int64_t chx_plan_block_words(const chx_plan *plan);
+int64_t chx_plan_input_bytes(const chx_plan *plan);
+int64_t chx_plan_sum_words(const chx_plan *plan);
+int64_t chx_plan_triangle_words(const chx_plan *plan);
+
+/* Fused correlator: exact visibilities of d_packed written into d_blocks in
+ * the reference block layout.  accumulate = 0 overwrites d_blocks, 1 adds
+ * to it.  Replaces the offsetAccumulateElements -> preseed -> corr chain of
+ * main_wrapper.c:693-777 (whose net result is the same buffer). */
+int chx_correlate(chx_plan *plan, const uint8_t *d_packed, int32_t *d_blocks,
+                  void *stream, int accumulate);
+
+/* Offset-binary nibble sums, uint32 [F][E][re, im] over T samples.
+ * Replaces offsetAccumulateElements (offset_accumulator.cl:7-49).
+ * accumulate = 0 zeroes d_sums first (main_wrapper.c:671-679 zeroes the
+ * buffer before every run); 1 adds like the reference's atomic_add. */
+int chx_offset_accumulate(chx_plan *plan, const uint8_t *d_packed,
+                          uint32_t *d_sums, void *stream, int accumulate);
+
+/* Writes (=) the offset correction into every block cell from the sums, for
+ * the plan's kernel_batch and convention.  Replaces preseed
+ * (preseed_multifreq_UT.cl:20-25, preseed_multifreq.cl,
+ * preseed_multifreq_highly_packed_correlator_method{_UT,}.cl). */
+int chx_preseed(chx_plan *plan, const uint32_t *d_sums, int32_t *d_blocks,
+                void *stream);
+
+/* Adds the reference corr kernel's partials (offset-domain products for the
+ * conference family, inverted-imaginary products for the packed family) to
+ * d_blocks, so that accumulate -> preseed -> corr_compat reproduces the
+ * reference pipeline bit for bit.  Replaces corr
+ * (pairwise_correlator_UT.cl:23-27,
+ * packed_correlator_overflow_protected_to_2272_iter_UT.cl:16-20).  Enforces
+ * the reference's own domain: T % time_accum == 0, time_accum % 8 == 0,
+ * T % 32 == 0, time_accum <= 291 (conference) or <= 2272 (packed), and
+ * F == 1 for the packed family (its kernel has no channel index). */
+int chx_corr_compat(chx_plan *plan, const uint8_t *d_packed, int32_t *d_blocks,
+                    void *stream);
+
+/* Block layout -> packed upper triangle int32 [F][E(E+1)/2][2], on the
+ * device.  Replaces the host reorganize_GPU_to_upper_triangle
+ * (gpu_data_reorg.c:76-124). */
+int chx_blocks_to_triangle(chx_plan *plan, const int32_t *d_blocks,
+                           int32_t *d_triangle, void *stream);
+
+/* Block layout -> full Hermitian matrix int32 [F][E][E][2] on the device.
+ * Replaces reorganize_GPU_to_full_Matrix_for_comparison
+ * (gpu_data_reorg.c:36-74). */
+int chx_blocks_to_full(chx_plan *plan, const int32_t *d_blocks, int32_t *d_full,
+                       void *stream);
+
+/* Reads and clears the plan's device error word (bounded-wait timeouts).
+ * Synchronises the stream.  Returns CHX_OK or CHX_E_TIMEOUT. */
+int chx_plan_check(chx_plan *plan, void *stream);
+
+/* ---------------------------------------------------------------------
+ * Batched ragged launch: many channels with their own element counts and
+ * sample counts in one persistent launch (captured in a CUDA graph).
+ * ------------------------------------------------------------------- */
+typedef struct chx_channel_desc {
+    int num_elements;      /* E_c, multiple of 32 */
+    int num_timesamples;   /* samples per integration, T_c */
+    int num_integrations;  /* integrations, each dumped to its own buffer */
+    int64_t input_stride;  /* bytes between consecutive samples (0 = E_c) */
+    const uint8_t *d_packed; /* [num_integrations * T_c] samples of E_c bytes */
+    int32_t *d_blocks;     /* num_integrations block buffers of NB_c*2048 */
+} chx_channel_desc;
+
+typedef struct chx_batch chx_batch;
+
+/* Builds the tile queue for n channels.  The descriptors are copied.  The
+ * channel work is ordered by a cost model; tile variant and sample splits
+ * come from the autotuner's cache (chx_autotune) when present. */
+int chx_batch_create(chx_batch **batch, int n, const chx_channel_desc *descs,
+                     int upper_triangle_convention, int device);
+/* Enqueues the whole batch (one graph launch).  accumulate as chx_correlate. */
+int chx_batch_run(chx_batch *batch, void *stream, int accumulate);
+/* Work units (tile pairs x splits) in the queue, and exact ops per run. */
+int64_t chx_batch_work_units(const chx_batch *batch);
+double chx_batch_ops(const chx_batch *batch);
+int chx_batch_destroy(chx_batch *batch);
+
+/* Times the tensor-core tile variants and split counts for (E, T) on the
+ * current device and caches the winner for chx_batch_create / AUTO plans.
+ * d_scratch_in/d_scratch_out must hold T*E bytes and NB*2048 int32. */
+int chx_autotune(int num_elements, int num_timesamples, const uint8_t *d_scratch_in,
+                 int32_t *d_scratch_out, void *stream, int *best_tile,
+                 int *best_split, double *best_ms);
+
+/* ---------------------------------------------------------------------
+ * Streaming: frames of samples arrive per channel; accumulators stay
+ * resident in HBM and are dumped every time_accum samples.
+ * ------------------------------------------------------------------- */
+typedef struct chx_stream chx_stream;
+
+typedef struct chx_stream_stats {
+    int64_t frames;         /* frames correlated */
+    int64_t dumps;          /* integrations completed */
+    double p50_ms, p99_ms;  /* frame-to-visibility latency percentiles */
+    double max_ms;
+    int64_t resident_bytes; /* HBM held by accumulators and dump buffers */
+} chx_stream_stats;
+
+/* hbm_budget_bytes = 0: admit while cudaMemGetInfo leaves headroom. */
+int chx_stream_create(chx_stream **s, int max_channels, int frame_len,
+                      int upper_triangle_convention, int64_t hbm_budget_bytes,
+                      int device);
+/* Admits a channel with E elements dumping every time_accum samples
+ * (a multiple of frame_len).  Returns CHX_E_ADMISSION when its resident
+ * accumulators (double buffered) do not fit the budget. */
+int chx_stream_admit(chx_stream *s, int num_elements, int time_accum,
+                     int *channel_id);
+/* Correlates one frame per listed channel (d_frames[i]: frame_len*E_c bytes
+ * on the device) in one launch; arrival_ns are the frames' host arrival
+ * times used for latency.  Completed integrations are swapped into the dump
+ * buffers. */
+int chx_stream_submit(chx_stream *s, int n, const int *channel_ids,
+                      const uint8_t *const *d_frames, const int64_t *arrival_ns,
+                      void *stream);
+/* Device pointer of channel c's last completed integration (NULL if none),
+ * and its sequence number. */
+int chx_stream_last_dump(chx_stream *s, int channel_id, const int32_t **d_blocks,
+                         int64_t *seq);
+/* Collects finished dump events and fills latency statistics. */
+int chx_stream_stats_get(chx_stream *s, chx_stream_stats *out);
+int chx_stream_destroy(chx_stream *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CHIMEX_H */

@@ -1,0 +1,210 @@
+"""GPU parity of libchimex against the CPU oracle, through the C ABI.
+
+Bit-exact integer comparisons: every output word must equal the oracle's.
+Small and golden cases compare whole buffers; the full BASELINE sizes use
+size-independent properties (weighted checksums over every element, exact
+constant-input values, random spot checks against O(T) direct sums).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as orc
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+KAT = json.load(open(os.path.join(GOLD, "kat.json")))["cases"]
+
+
+@pytest.fixture(scope="module")
+def chimex():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import chimex as cx
+    return cx
+
+
+ALGOS = ["simt", "tc"]
+
+
+def make_plan(cx, E, F, T, TA=256, ut=1, kb=0, algo="auto", tsplit=0):
+    p = cx.Plan(E, F, T, TA, ut, kb, 0)
+    if algo == "simt":
+        p.set_option(cx.OPT_ALGO, cx.ALGO_SIMT)
+    elif algo == "tc":
+        try:
+            p.set_option(cx.OPT_ALGO, cx.ALGO_TC)
+        except cx.ChimexError as e:
+            if e.code == cx.E_UNSUPPORTED:
+                pytest.skip("tensor-core path not available for this shape")
+            raise
+    if tsplit:
+        p.set_option(cx.OPT_TSPLIT, tsplit)
+    return p
+
+
+def to_dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def gpu_blocks(cx, packed, E, F, T, ut=1, algo="auto", tsplit=0):
+    p = make_plan(cx, E, F, T, ut=ut, algo=algo, tsplit=tsplit)
+    out = p.correlate(to_dev(packed))
+    p.check_device()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("case", KAT, ids=[c["key"] for c in KAT])
+def test_golden_cases(chimex, case, algo):
+    T, F, E, ut = case["T"], case["F"], case["E"], case["ut"]
+    packed = orc.generate(T, F, E, case["gen"], case["seed"], case["default_re"],
+                          case["default_im"], case["initial_re"], case["initial_im"],
+                          case["single_freq"], case["no_repeat"])
+    blocks = gpu_blocks(chimex, packed, E, F, T, ut, algo)
+    tri = orc.blocks_to_triangle(blocks, F, E)
+    assert orc.fnv1a(tri) == case["tri_fnv"]
+    if E <= 256:
+        np.testing.assert_array_equal(blocks, orc.correlate_blocks(packed, T, F, E, ut))
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("E,F,T,ut", [
+    (32, 1, 1, 1), (32, 1, 3, 0), (64, 2, 31, 1), (96, 3, 17, 1), (128, 1, 129, 0),
+    (160, 2, 200, 1), (224, 1, 64, 1), (384, 1, 100, 1), (640, 2, 48, 0),
+])
+def test_edge_shapes(chimex, algo, E, F, T, ut):
+    packed = orc.generate(T, F, E, 4, 1000 + E + T, no_repeat=1)
+    blocks = gpu_blocks(chimex, packed, E, F, T, ut, algo)
+    np.testing.assert_array_equal(blocks, orc.correlate_blocks(packed, T, F, E, ut))
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_extreme_values(chimex, algo):
+    """All 256 byte values as elements; constant -8 is the int32 worst case."""
+    T, F, E = 40, 1, 256
+    packed = np.tile(np.arange(256, dtype=np.uint8), T)
+    blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
+    np.testing.assert_array_equal(blocks, orc.correlate_blocks(packed, T, F, E, 1))
+    T = 2048
+    packed = np.zeros(T * 128, dtype=np.uint8)  # re = im = -8 everywhere
+    blocks = gpu_blocks(chimex, packed, 128, 1, T, 1, algo)
+    assert (blocks[0::2] == 128 * T).all() and (blocks[1::2] == 0).all()
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+@pytest.mark.parametrize("tsplit", [1, 2, 3, 7])
+def test_sample_splits_and_accumulate(chimex, algo, tsplit):
+    T, F, E = 300, 2, 128
+    packed = orc.generate(T, F, E, 4, 77, no_repeat=1)
+    ref = orc.correlate_blocks(packed, T, F, E, 1)
+    p = make_plan(chimex, E, F, T, algo=algo, tsplit=tsplit)
+    d = to_dev(packed)
+    out = p.correlate(d)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+    p.correlate(d, out, accumulate=True)
+    np.testing.assert_array_equal(out.cpu().numpy(), (ref.astype(np.int64) * 2).astype(np.int32))
+
+
+def test_offset_accumulate_and_preseed(chimex):
+    T, F, E = 96, 3, 96
+    packed = orc.generate(T, F, E, 4, 5, no_repeat=1)
+    for kb in (0, 1):
+        for ut in (0, 1):
+            p = chimex.Plan(E, F, T, 32, ut, kb, 0)
+            d = to_dev(packed)
+            sums = p.offset_accumulate(d)
+            np.testing.assert_array_equal(sums.cpu().numpy().view(np.uint32),
+                                          orc.offset_accumulate(packed, T, F, E))
+            blocks = p.preseed(sums)
+            ref = orc.preseed(orc.offset_accumulate(packed, T, F, E), T, F, E, kb, ut)
+            np.testing.assert_array_equal(blocks.cpu().numpy(), ref)
+            # accumulate=1 adds to the existing sums like the reference atomic_add
+            p.offset_accumulate(d, sums, accumulate=True)
+            np.testing.assert_array_equal(sums.cpu().numpy().view(np.uint32),
+                                          2 * orc.offset_accumulate(packed, T, F, E))
+
+
+@pytest.mark.parametrize("kb,ut,F,TA", [(0, 1, 3, 256), (0, 0, 2, 288), (0, 1, 1, 8),
+                                          (1, 1, 1, 1912), (1, 0, 1, 256)])
+def test_reference_pipeline_compat(chimex, kb, ut, F, TA):
+    """accumulate -> preseed -> corr_compat reproduces the reference pipeline:
+    the preseed values and the corr partials each match the oracle's
+    restatement of the reference kernels, and their sum is exact."""
+    E = 128
+    T = TA * 2
+    while T % 32:
+        T += TA
+    packed = orc.generate(T, F, E, 4, 9, no_repeat=1)
+    p = chimex.Plan(E, F, T, TA, ut, kb, 0)
+    d = to_dev(packed)
+    zero = torch.zeros(p.block_words, dtype=torch.int32, device="cuda")
+    partial = p.corr_compat(d, zero).cpu().numpy()
+    np.testing.assert_array_equal(partial, orc.corr_partials(packed, T, F, E, kb, ut))
+    full = p.reference_pipeline(d).cpu().numpy()
+    np.testing.assert_array_equal(full, orc.correlate_blocks(packed, T, F, E, ut))
+
+
+@pytest.mark.parametrize("kb,F,T,TA", [(0, 1, 592, 296), (0, 1, 100, 20), (0, 1, 120, 12),
+                                         (1, 2, 512, 256), (1, 1, 4608, 2304)])
+def test_compat_rejects_outside_reference_domain(chimex, kb, F, T, TA):
+    p = chimex.Plan(64, F, T, TA, 1, kb, 0)
+    d = torch.zeros(p.input_bytes, dtype=torch.uint8, device="cuda")
+    out = torch.zeros(p.block_words, dtype=torch.int32, device="cuda")
+    with pytest.raises(chimex.ChimexError) as ei:
+        p.corr_compat(d, out)
+    assert ei.value.code in (chimex.E_INVALID, chimex.E_UNSUPPORTED)
+
+
+def test_reorg_kernels(chimex):
+    T, F, E = 32, 2, 96
+    packed = orc.generate(T, F, E, 4, 8, no_repeat=1)
+    p = chimex.Plan(E, F, T, 32, 1, 0, 0)
+    blocks = p.correlate(to_dev(packed))
+    ref_blocks = orc.correlate_blocks(packed, T, F, E, 1)
+    np.testing.assert_array_equal(p.blocks_to_triangle(blocks).cpu().numpy(),
+                                  orc.blocks_to_triangle(ref_blocks, F, E))
+    np.testing.assert_array_equal(p.blocks_to_full(blocks).cpu().numpy(),
+                                  orc.blocks_to_full(ref_blocks, F, E))
+
+
+def _checksums(packed, blocks, T, F, E, seed, nspot=64):
+    rng = np.random.default_rng(seed)
+    for f in range(F):
+        w = rng.integers(-3, 4, size=2 * E).astype(np.int32)
+        assert orc.weighted_power(packed, T, F, E, f, w) == \
+            orc.weighted_from_blocks(blocks, F, E, f, w), "checksum of channel %d" % f
+        for _ in range(nspot):
+            y = int(rng.integers(0, E))
+            x = int(rng.integers(32 * (y // 32), E))
+            off = orc.block_cell_offset(E, f, y, x)
+            assert orc.visibility(packed, T, F, E, f, y, x) == \
+                (blocks[off], blocks[off + 1]), (f, y, x)
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_full_size_plain_config(chimex, algo):
+    """E=2048, F=8, T=16384, random no-repeat."""
+    E, F, T = 2048, 8, 16384
+    packed = orc.generate(T, F, E, 4, 42, no_repeat=1)
+    blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
+    _checksums(packed, blocks, T, F, E, seed=1)
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_full_size_overflow_edge_config(chimex, algo):
+    """E=2048, F=16, T=1912*8; channels 0-7 constant -8
+    (|Re| = 128 T, the int32 worst case), channels 8-15 seeded random."""
+    E, F, T = 2048, 16, 1912 * 8
+    const = orc.generate(T, 8, E, 1, 42, initial_re=-8, initial_im=-8)
+    rnd = orc.generate(T, 8, E, 4, 42, no_repeat=1)
+    packed = np.concatenate([const.reshape(T, 8, E), rnd.reshape(T, 8, E)], axis=1).ravel()
+    blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
+    nbw = orc.num_blocks(E) * 2048
+    head = blocks[: 8 * nbw]
+    assert (head[0::2] == 128 * T).all() and (head[1::2] == 0).all()
+    _checksums(packed, blocks, T, F, E, seed=2, nspot=16)
