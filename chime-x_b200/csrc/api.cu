@@ -154,8 +154,14 @@ int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void 
         a.T = p->T;
         a.map = MAP_EXACT;
         a.ut = p->ut;
-        a.splits = p->tsplit;  // 0 = let the launcher decide
-        a.mode = accumulate ? 1 : 0;
+        a.splits = p->tsplit ? p->tsplit : 1;
+        if (a.splits > 1) {
+            if (!accumulate)
+                CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)chx_plan_block_words(p) * 4, st));
+            a.mode = 2;
+        } else {
+            a.mode = accumulate ? 1 : 0;
+        }
         a.err = p->d_err;
         CHX_CUDA(launch_correlate_tc(a, p->sm_count, st));
         return CHX_OK;
@@ -216,6 +222,24 @@ int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, voi
     DeviceGuard g(p->device);
     cudaStream_t st = (cudaStream_t)stream;
     const int map = p->kernel_batch == CHX_KERNEL_PACKED ? MAP_PACKED : MAP_CONF;
+    if (p->algo != CHX_ALGO_SIMT && tc_supported(p->E, p->T)) {
+        TcArgs a;
+        a.packed = d_packed;
+        a.in_stride = (int64_t)p->F * p->E;
+        a.chan_stride = p->E;
+        a.blocks = d_blocks;
+        a.out_chan_stride = p->NB * 2048;
+        a.E = p->E;
+        a.F = p->F;
+        a.T = p->T;
+        a.map = map;
+        a.ut = p->ut;
+        a.splits = p->tsplit ? p->tsplit : 1;
+        a.mode = a.splits > 1 ? 2 : 1;
+        a.err = p->d_err;
+        CHX_CUDA(launch_correlate_tc(a, p->sm_count, st));
+        return CHX_OK;
+    }
     const int splits =
         p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);
     CHX_CUDA(launch_correlate_simt(d_packed, d_blocks, p->E, p->F, p->T, map, p->ut,

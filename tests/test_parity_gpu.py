@@ -129,9 +129,10 @@ def test_offset_accumulate_and_preseed(chimex):
                                           2 * orc.offset_accumulate(packed, T, F, E))
 
 
+@pytest.mark.parametrize("algo", ALGOS)
 @pytest.mark.parametrize("kb,ut,F,TA", [(0, 1, 3, 256), (0, 0, 2, 288), (0, 1, 1, 8),
                                           (1, 1, 1, 1912), (1, 0, 1, 256)])
-def test_reference_pipeline_compat(chimex, kb, ut, F, TA):
+def test_reference_pipeline_compat(chimex, kb, ut, F, TA, algo):
     """accumulate -> preseed -> corr_compat reproduces the reference pipeline:
     the preseed values and the corr partials each match the oracle's
     restatement of the reference kernels, and their sum is exact."""
@@ -140,7 +141,7 @@ def test_reference_pipeline_compat(chimex, kb, ut, F, TA):
     while T % 32:
         T += TA
     packed = orc.generate(T, F, E, 4, 9, no_repeat=1)
-    p = chimex.Plan(E, F, T, TA, ut, kb, 0)
+    p = make_plan(chimex, E, F, T, TA, ut, kb, algo)
     d = to_dev(packed)
     zero = torch.zeros(p.block_words, dtype=torch.int32, device="cuda")
     partial = p.corr_compat(d, zero).cpu().numpy()
