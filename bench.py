@@ -69,7 +69,7 @@ def int8_peak(peaks):
 class ClockSampler:
     """Samples SM clocks and throttle reasons with nvidia-smi while running."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -97,6 +97,12 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
     def summary(self):
         if self.proc is None or self.tmp is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -108,6 +114,18 @@ class ClockSampler:
                 if len(parts) >= 9:
                     rows.append(parts)
         os.unlink(self.tmp.name)
+        import datetime
+        t0, t1 = getattr(self, "t0", None), getattr(self, "t1", None)
+        if t0 is not None and t1 is not None:
+            keep = []
+            for r in rows:
+                try:
+                    ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    continue
+                if t0 - 0.05 <= ts <= t1 + 0.05:
+                    keep.append(r)
+            rows = keep
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         def num(x):
@@ -194,7 +212,7 @@ def run_reference_arm(args):
 # --------------------------------------------------------------- our arm
 def run_plain(args, torch, cx, dist):
     rank, local_rank, world = env_rank()
-    E, F, T, TA = 2048, 8, 16384, 256
+    E, F, T, TA = args.E, args.F, args.T, 256
     dev = torch.device("cuda", local_rank)
     plan = cx.Plan(E, F, T, TA, 1, 0, local_rank)
     if args.algo == "simt":
@@ -218,17 +236,17 @@ def run_plain(args, torch, cx, dist):
         if dist is not None:
             dist.barrier()
 
-    for _ in range(max(args.warmup, 3)):
-        step()
-    plan.check_device()
-    torch.cuda.synchronize(dev)
-
-    # device-timed region: inputs (256 MiB) are larger than L2 (126 MB)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    barrier()
-    torch.cuda.synchronize(dev)
     with ClockSampler(local_rank) as clk:
+        for _ in range(max(args.warmup, 3)):
+            step()
+        plan.check_device()
+        torch.cuda.synchronize(dev)
+        # device-timed region: inputs larger than L2 (see config["l2"])
+        barrier()
+        torch.cuda.synchronize(dev)
+        clk.mark_start()
         t_start = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
         t_start.record(stream)
@@ -238,6 +256,7 @@ def run_plain(args, torch, cx, dist):
             ev[k][1].record(stream)
         t_end.record(stream)
         torch.cuda.synchronize(dev)
+        clk.mark_end()
     barrier()
     plan.check_device()
     total_ms = t_start.elapsed_time(t_end)
@@ -272,10 +291,11 @@ def run_plain(args, torch, cx, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
         "data": "synthetic: seeded uniform 4-bit complex (re, im uniform in [-8, 7]), "
                 "device-generated",
-        "config": {"workload": "plain correlator E=2048 F=8 T=16384 time_accum=256 per GPU, "
-                               "one chx_correlate launch per step",
+        "config": {"workload": "plain correlator E=%d F=%d T=%d time_accum=256 per GPU, "
+                               "one chx_correlate launch per step" % (E, F, T),
                    "E": E, "F": F, "T": T, "time_accum": TA, "algo": args.algo,
-                   "l2": "inputs (256 MiB) larger than L2 (126 MB); no flush",
+                   "l2": "inputs (%d MiB) %s L2 (126 MB); no flush" % (
+                       E * F * T >> 20, "larger than" if E * F * T > 126e6 else "SMALLER than"),
                    "parallelism": "channel shards, %d GPU(s), no collective" % world},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
                      "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
@@ -363,8 +383,11 @@ def run_e2e(args, torch, cx, plan, dev, ops_step, world, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--E", type=int, default=2048, help="elements (profiling cases)")
+    ap.add_argument("--F", type=int, default=8, help="channels per GPU (profiling cases)")
+    ap.add_argument("--T", type=int, default=16384, help="samples (profiling cases)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="plain", choices=["plain", "batched", "stream"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "tc"])

@@ -28,6 +28,76 @@ void clear_error() { g_err[0] = 0; }
 
 using namespace chx;
 
+namespace {
+
+void free_plan_device(chx_plan *p) {
+    if (p->d_err) cudaFree(p->d_err);
+    if (p->d_chans) cudaFree(p->d_chans);
+    if (p->d_units) cudaFree(p->d_units);
+    p->d_err = nullptr;
+    p->d_chans = nullptr;
+    p->d_units = nullptr;
+}
+
+// Channel table and work units of the tensor-core kernel for the plan's
+// shape: F channels sharing one TMA map (passed per launch), units of every
+// channel sorted by decreasing cost.
+cudaError_t build_tc_tables(chx_plan *p) {
+    std::vector<ChanDesc> chans(p->F);
+    memset(chans.data(), 0, chans.size() * sizeof(ChanDesc));
+    for (int f = 0; f < p->F; f++) {
+        chans[f].out = (uint64_t)f * (uint64_t)p->NB * 2048u * 4u;
+        chans[f].E = p->E;
+        chans[f].nb1 = (int)p->NB1;
+        chans[f].fcoord = f;
+    }
+    std::vector<Unit> units;
+    for (int f = 0; f < p->F; f++) tc_append_units(units, f, p->E, 0, p->T, p->tsplit, 0);
+    tc_sort_units(units);
+    if (p->d_chans) cudaFree(p->d_chans);
+    if (p->d_units) cudaFree(p->d_units);
+    p->d_chans = p->d_units = nullptr;
+    cudaError_t e = cudaMalloc(&p->d_chans, chans.size() * sizeof(ChanDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_units, units.size() * sizeof(Unit));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->d_chans, chans.data(), chans.size() * sizeof(ChanDesc),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(p->d_units, units.data(), units.size() * sizeof(Unit),
+                       cudaMemcpyHostToDevice);
+    p->nunits = (int)units.size();
+    p->has_split_units = false;
+    for (const Unit &u : units) p->has_split_units |= (u.split != 0);
+    return e;
+}
+
+// Launches the tensor-core kernel on the plan's tables with `map`.
+int run_tc(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, int map, int accumulate,
+           cudaStream_t st) {
+    if ((reinterpret_cast<uintptr_t>(d_packed) & 15) != 0)
+        return fail(CHX_E_INVALID, "packed input must be 16-byte aligned for TMA");
+    CUtensorMap tmap;
+    const int r = tc_encode_map(&tmap, d_packed, p->E, p->F, p->T, p->E, (int64_t)p->F * p->E);
+    if (r != 0) return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", r);
+    if (p->has_split_units && !accumulate)
+        CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)chx_plan_block_words(p) * 4, st));
+    TcLaunch L;
+    L.chans = (const ChanDesc *)p->d_chans;
+    L.units = (const Unit *)p->d_units;
+    L.nunits = p->nunits;
+    L.out_base = (uint64_t)d_blocks;
+    L.use_param_map = 1;
+    L.map = map;
+    L.ut = p->ut;
+    L.accumulate = accumulate;
+    L.err = p->d_err;
+    L.grid = p->nunits < p->sm_count ? p->nunits : p->sm_count;
+    CHX_CUDA(tc_launch(L, &tmap, st));
+    return CHX_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *chx_version(void) { return "chimex-b200 0.1"; }
@@ -71,11 +141,15 @@ int chx_plan_create(chx_plan **plan, int E, int F, int T, int TA, int ut, int ke
     p->tsplit = 0;
     p->tile = 0;
     p->d_err = nullptr;
+    p->d_chans = nullptr;
+    p->d_units = nullptr;
+    p->nunits = 0;
     cudaError_t e = cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = build_tc_tables(p);
     if (e != cudaSuccess) {
-        if (p->d_err) cudaFree(p->d_err);
+        free_plan_device(p);
         delete p;
         return cuda_fail(e, "plan device state");
     }
@@ -87,7 +161,7 @@ int chx_plan_destroy(chx_plan *p) {
     clear_error();
     if (!p) return CHX_OK;
     DeviceGuard g(p->device);
-    if (p->d_err) cudaFree(p->d_err);
+    free_plan_device(p);
     delete p;
     return CHX_OK;
 }
@@ -103,10 +177,13 @@ int chx_plan_set_option(chx_plan *p, int option, int64_t value) {
             return fail(CHX_E_UNSUPPORTED, "tensor-core path does not take E=%d T=%d", p->E, p->T);
         p->algo = (int)value;
         return CHX_OK;
-    case CHX_OPT_TSPLIT:
+    case CHX_OPT_TSPLIT: {
         if (value < 0 || value > 4096) return fail(CHX_E_INVALID, "tsplit %lld", (long long)value);
         p->tsplit = (int)value;
+        DeviceGuard g(p->device);
+        CHX_CUDA(build_tc_tables(p));
         return CHX_OK;
+    }
     case CHX_OPT_TILE:
         if (value < 0 || value > 16) return fail(CHX_E_INVALID, "tile %lld", (long long)value);
         p->tile = (int)value;
@@ -142,30 +219,7 @@ int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void 
     cudaStream_t st = (cudaStream_t)stream;
     const bool use_tc =
         (p->algo == CHX_ALGO_TC) || (p->algo == CHX_ALGO_AUTO && tc_supported(p->E, p->T));
-    if (use_tc) {
-        TcArgs a;
-        a.packed = d_packed;
-        a.in_stride = (int64_t)p->F * p->E;
-        a.chan_stride = p->E;
-        a.blocks = d_blocks;
-        a.out_chan_stride = p->NB * 2048;
-        a.E = p->E;
-        a.F = p->F;
-        a.T = p->T;
-        a.map = MAP_EXACT;
-        a.ut = p->ut;
-        a.splits = p->tsplit ? p->tsplit : 1;
-        if (a.splits > 1) {
-            if (!accumulate)
-                CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)chx_plan_block_words(p) * 4, st));
-            a.mode = 2;
-        } else {
-            a.mode = accumulate ? 1 : 0;
-        }
-        a.err = p->d_err;
-        CHX_CUDA(launch_correlate_tc(a, p->sm_count, st));
-        return CHX_OK;
-    }
+    if (use_tc) return run_tc(p, d_packed, d_blocks, MAP_EXACT, accumulate ? 1 : 0, st);
     const int splits =
         p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);
     int mode;
@@ -222,24 +276,8 @@ int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, voi
     DeviceGuard g(p->device);
     cudaStream_t st = (cudaStream_t)stream;
     const int map = p->kernel_batch == CHX_KERNEL_PACKED ? MAP_PACKED : MAP_CONF;
-    if (p->algo != CHX_ALGO_SIMT && tc_supported(p->E, p->T)) {
-        TcArgs a;
-        a.packed = d_packed;
-        a.in_stride = (int64_t)p->F * p->E;
-        a.chan_stride = p->E;
-        a.blocks = d_blocks;
-        a.out_chan_stride = p->NB * 2048;
-        a.E = p->E;
-        a.F = p->F;
-        a.T = p->T;
-        a.map = map;
-        a.ut = p->ut;
-        a.splits = p->tsplit ? p->tsplit : 1;
-        a.mode = a.splits > 1 ? 2 : 1;
-        a.err = p->d_err;
-        CHX_CUDA(launch_correlate_tc(a, p->sm_count, st));
-        return CHX_OK;
-    }
+    if (p->algo != CHX_ALGO_SIMT && tc_supported(p->E, p->T))
+        return run_tc(p, d_packed, d_blocks, map, 1, st);
     const int splits =
         p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);
     CHX_CUDA(launch_correlate_simt(d_packed, d_blocks, p->E, p->F, p->T, map, p->ut,

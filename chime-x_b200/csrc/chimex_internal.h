@@ -1,10 +1,12 @@
 // chimex_internal.h -- shared declarations of libchimex (not installed).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/chimex.h"
 
@@ -40,6 +42,10 @@ struct chx_plan {
     int tile;     // 0 = auto
     int *d_err;   // device error word (bounded-wait timeouts)
     int sm_count;
+    void *d_chans;  // tensor-core channel table (ChanDesc[F])
+    void *d_units;  // tensor-core work units (Unit[nunits])
+    int nunits;
+    bool has_split_units;  // some output cells receive several units (atomic)
 };
 
 namespace chx {
@@ -90,20 +96,55 @@ cudaError_t launch_blocks_to_triangle(const int32_t *blocks, int32_t *tri, int E
 cudaError_t launch_blocks_to_full(const int32_t *blocks, int32_t *full, int E, int F,
                                   cudaStream_t st);
 
-// ---- tensor-core kernels (tc_correlator.cu) ----
-struct TcArgs {
-    const uint8_t *packed;  // [T][F][E] (sample stride = in_stride bytes)
-    int64_t in_stride;      // bytes between consecutive samples of a channel
-    int64_t chan_stride;    // bytes between channels within a sample row
-    int32_t *blocks;        // [F][NB][2048]
-    int64_t out_chan_stride;  // int32 words between channels' block buffers
-    int E, F, T;
-    int map, ut;
-    int mode;       // 0 store, 1 add, 2 atomic add
-    int splits;     // sample-range splits
-    int *err;       // device error word
+// ---- tensor-core kernel (tc_correlator.cu) ----
+// A channel as the tensor-core kernel sees it: the TMA map of its packed
+// samples (dims {E, channels, samples}), its block-buffer address and shape.
+struct __align__(64) ChanDesc {
+    CUtensorMap map;  // used unless the launch passes one map for all channels
+    uint64_t out;     // block buffer: absolute address, or byte offset added to
+                      // the launch's out_base
+    int E;            // elements
+    int nb1;          // E / 32
+    int fcoord;       // channel coordinate inside the TMA map
+    int pad[11];
 };
+static_assert(sizeof(ChanDesc) == 192, "ChanDesc layout");
+
+// One work unit: a 128-element y tile against one or two 128-element x tiles
+// of one channel over samples [t0, t1).  tyx = ty | x0 << 10 | nx << 20.
+struct Unit {
+    int chan;
+    int tyx;
+    int t0, t1;
+    long long out_off;  // int32 words added to the channel's block buffer
+    int split;          // 1: other units add to the same cells (atomic add)
+    int cost;           // samples x x-tiles, for scheduling
+};
+static_assert(sizeof(Unit) == 32, "Unit layout");
+
+constexpr int kUnitMaxSamples = 1 << 18;  // int32-exact bound per unit
+
+struct TcLaunch {
+    const ChanDesc *chans;  // device
+    const Unit *units;      // device, sorted by decreasing cost
+    int nunits;
+    uint64_t out_base;      // added to ChanDesc::out
+    int use_param_map;      // 1: every channel uses the kernel-parameter map
+    int map;                // value map (MAP_*)
+    int ut;
+    int accumulate;
+    int *err;
+    int grid;               // persistent CTAs (<= SMs)
+};
+
 bool tc_supported(int E, int T);
-cudaError_t launch_correlate_tc(const TcArgs &a, int sm_count, cudaStream_t st);
+// Appends the units of one channel's sample range [t_begin, t_end) to `out`.
+void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t_end,
+                     int tsplit, long long out_off);
+void tc_sort_units(std::vector<Unit> &u);
+// Encodes the TMA map of packed samples: dims {E, channels, samples}.
+int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
+                  int64_t chan_stride, int64_t sample_stride);
+cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st);
 
 }  // namespace chx

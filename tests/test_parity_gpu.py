@@ -209,3 +209,21 @@ def test_full_size_overflow_edge_config(chimex, algo):
     head = blocks[: 8 * nbw]
     assert (head[0::2] == 128 * T).all() and (head[1::2] == 0).all()
     _checksums(packed, blocks, T, F, E, seed=2, nspot=16)
+
+
+@pytest.mark.parametrize("E,F,T", [(2048, 16, 4096), (1024, 16, 15296), (2048, 32, 2048)])
+def test_tc_repeatable_against_simt(chimex, E, F, T):
+    """Persistent tensor-core launches over many units, repeated: every run
+    must equal the CUDA-core kernel bit for bit (catches pipeline races that a
+    single run can miss).  The CUDA-core kernel is itself pinned to the oracle
+    by the tests above."""
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(E + F + T)
+    d = torch.randint(0, 256, (T * F * E,), dtype=torch.uint8, device="cuda", generator=gen)
+    ref = make_plan(chimex, E, F, T, algo="simt").correlate(d)
+    p = make_plan(chimex, E, F, T, algo="tc")
+    out = torch.empty_like(ref)
+    for _ in range(4):
+        p.correlate(d, out)
+        p.check_device()
+        assert torch.equal(out, ref)
