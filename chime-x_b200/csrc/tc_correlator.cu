@@ -19,11 +19,13 @@
 // Shared-memory operands are MN-major (elements contiguous, like the input
 // bytes) with the 128-byte swizzle: an 8 k-row x 128-byte atom per 8 samples
 // and component.  One stage covers 32 samples:
-//   y: atoms [R0 I0 R1 I1 R2 I2 R3 I3 | N0 N1 N2 N3]        12 KiB
-//   x: per 128-element slice [X0 Y0 X1 Y1 X2 Y2 X3 Y3]      8 KiB per slice
-// (digit = 8-sample block).  Four MMAs per stage (K = 32 each):
-//   Re: A = R0 I0 R1 I1 (SBO 1K) with X0 Y0 X1 Y1;  A = R2 I2 R3 I3 with X2 Y2 X3 Y3
-//   Im: A = I0..I3 (SBO 2K) with X0..X3 (SBO 2K);   A = N0..N3 with Y0..Y3
+//   y: atoms [R0 I0 R1 I1 R2 I2 R3 I3 | I0 N0 I1 N1 I2 N2 I3 N3]   16 KiB
+//   x: per 128-element slice [X0 Y0 X1 Y1 X2 Y2 X3 Y3]             8 KiB per slice
+// (digit = 8-sample block; the I rows are stored twice so that every MMA
+// reads four consecutive atoms).  Four MMAs per stage (K = 32 each),
+// alternating accumulators so that consecutive MMAs are independent:
+//   Re += [R0 I0 R1 I1].[X0 Y0 X1 Y1]    Im += [I0 N0 I1 N1].[X0 Y0 X1 Y1]
+//   Re += [R2 I2 R3 I3].[X2 Y2 X3 Y3]    Im += [I2 N2 I3 N3].[X2 Y2 X3 Y3]
 //
 // Roles (320 threads, one persistent CTA per SM, units taken round-robin from
 // a table sorted by decreasing cost):
@@ -48,7 +50,7 @@ namespace {
 constexpr int kStageSamples = 32;
 constexpr int kOpStages = 4;    // operand ring
 constexpr int kPkStages = 6;    // packed-tile ring
-constexpr int kYOpBytes = 12 * 1024;
+constexpr int kYOpBytes = 16 * 1024;
 constexpr int kXOpBytes = 16 * 1024;
 constexpr int kPkYBytes = kStageSamples * 128;      // 4 KiB
 constexpr int kPkXBytes = 2 * kPkYBytes;            // 8 KiB
@@ -358,6 +360,12 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
             uint32_t g = 0, acc_phase = 0;
             bool ok = true;
             const bool b_signed = (MAP == MAP_EXACT);
+            // Descriptors of operand slot 0; slot s adds its byte offset >> 4
+            // to the start-address field (shared addresses stay < 256 KiB).
+            const uint64_t dRe0 = sdesc(op_y, 1024, 1024), dRe1 = sdesc(op_y + 4096, 1024, 1024);
+            const uint64_t dIm0 = sdesc(op_y + 8192, 1024, 1024);
+            const uint64_t dIm1 = sdesc(op_y + 12288, 1024, 1024);
+            const uint64_t dX0 = sdesc(op_x, 8192, 1024), dX1 = sdesc(op_x + 4096, 8192, 1024);
             for (int u = first; u < nunits && ok; u += stride) {
                 const Unit U = P.units[u];
                 const int nx = (U.tyx >> 20) & 3;
@@ -378,18 +386,13 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t ya = op_y + s * kYOpBytes, xa = op_x + s * kXOpBytes;
+                    const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
+                    const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
                     const uint32_t first_k = (it > 0) ? 1u : 0u;
-                    // Re += R*X + I*Y
-                    mma_i8(tmem_base, sdesc(ya, 1024, 1024), sdesc(xa, 8192, 1024), idesc,
-                           first_k);
-                    mma_i8(tmem_base, sdesc(ya + 4096, 1024, 1024), sdesc(xa + 4096, 8192, 1024),
-                           idesc, 1u);
-                    // Im += I*X + N*Y
-                    mma_i8(tmem_base + 256, sdesc(ya + 1024, 1024, 2048), sdesc(xa, 8192, 2048),
-                           idesc, first_k);
-                    mma_i8(tmem_base + 256, sdesc(ya + 8192, 1024, 1024),
-                           sdesc(xa + 1024, 8192, 2048), idesc, 1u);
+                    mma_i8(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, first_k);        // Re
+                    mma_i8(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, first_k);  // Im
+                    mma_i8(tmem_base, dRe1 + so_y, dX1 + so_x, idesc, 1u);             // Re
+                    mma_i8(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);       // Im
                     // Release the operand slot unless nothing will refill it:
                     // no arrival may be left pending when the CTA retires.
                     if (!(last_unit && it + kOpStages >= nst)) mma_commit(empty_op(s));
@@ -413,8 +416,8 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         const int sy = tid >> 3, gy = tid & 7;
         const uint32_t ry = (uint32_t)(sy & 7), by8 = (uint32_t)(sy >> 3);
         const uint32_t ldy = (uint32_t)(sy * 128 + gy * 16);
-        const uint32_t sty_r = (2 * by8) * 1024 + swz(ry, gy);
-        const uint32_t sty_n = 8192 + by8 * 1024 + swz(ry, gy);
+        const uint32_t sty_r = (2 * by8) * 1024 + swz(ry, gy);  // R; I at +1K
+        const uint32_t sty_i = 8192 + sty_r;                      // I; N at +1K
         // x chunks c = tid + 256 j (slice j): the same sample and group as y
         const uint32_t stx = (2 * by8) * 1024 + swz(ry, gy);
         uint32_t g = 0, acc_phase = 0;
@@ -468,7 +471,8 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                 const uint32_t ya = op_y + os * kYOpBytes, xa = op_x + os * kXOpBytes;
                 sts128(ya + sty_r, r[0], r[1], r[2], r[3]);
                 sts128(ya + sty_r + 1024, i[0], i[1], i[2], i[3]);
-                sts128(ya + sty_n, n[0], n[1], n[2], n[3]);
+                sts128(ya + sty_i, i[0], i[1], i[2], i[3]);
+                sts128(ya + sty_i + 1024, n[0], n[1], n[2], n[3]);
                 sts128(xa + stx, xr0[0], xr0[1], xr0[2], xr0[3]);
                 sts128(xa + stx + 1024, xi0[0], xi0[1], xi0[2], xi0[3]);
                 if (nx > 1) {
