@@ -27,13 +27,16 @@
 //   Re += [R0 I0 R1 I1].[X0 Y0 X1 Y1]    Im += [I0 N0 I1 N1].[X0 Y0 X1 Y1]
 //   Re += [R2 I2 R3 I3].[X2 Y2 X3 Y3]    Im += [I2 N2 I3 N3].[X2 Y2 X3 Y3]
 //
-// Roles (320 threads, one persistent CTA per SM, units taken round-robin from
+// Roles (576 threads, one persistent CTA per SM, units taken round-robin from
 // a table sorted by decreasing cost):
-//   warps 0-7  unpack: read packed bytes from the TMA ring, convert with SWAR
-//              logic, store swizzled operand rows; then the epilogue (TMEM ->
-//              reference block layout).
-//   warp 8     TMA producer: packed y and x tiles, 32 samples per stage.
-//   warp 9     TMEM allocation and the single-thread MMA issue loop.
+//   warps 0-15 unpack: read packed bytes from the TMA ring, convert with SWAR
+//              logic, store swizzled operand rows (warps 0-7 the y tile,
+//              8-15 the x tile); then the epilogue (TMEM -> block layout).
+//   warp 16    TMA producer: packed y and x tiles, 32 samples per stage.
+//   warp 17    TMEM allocation and the single-thread MMA issue loop, which
+//              consumes stages in pairs (four Re MMAs, four Im MMAs, one
+//              commit) because switching accumulators or committing after
+//              every few MMAs stalls the tensor pipe.
 // Every wait is bounded (globaltimer): on timeout the CTA records an error
 // code in the caller's error word, drains its MMAs and TMA loads and returns.
 #include "chimex_internal.h"
@@ -54,11 +57,11 @@ constexpr int kYOpBytes = 16 * 1024;
 constexpr int kXOpBytes = 16 * 1024;
 constexpr int kPkYBytes = kStageSamples * 128;      // 4 KiB
 constexpr int kPkXBytes = 2 * kPkYBytes;            // 8 KiB
-constexpr int kUnpackWarps = 8;
+constexpr int kUnpackWarps = 16;
 constexpr int kUnpackThreads = kUnpackWarps * 32;
-constexpr int kProducerWarp = 8;
-constexpr int kMmaWarp = 9;
-constexpr int kThreads = 320;
+constexpr int kProducerWarp = 16;
+constexpr int kMmaWarp = 17;
+constexpr int kThreads = 576;
 constexpr int kTmemCols = 512;
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
 
@@ -173,17 +176,13 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-          "=r"(r[31])
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() {
@@ -270,16 +269,16 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
     const uint32_t op_y = sbase + kOffOpY, op_x = sbase + kOffOpX;
     const uint32_t pk_y = sbase + kOffPkY, pk_x = sbase + kOffPkX;
     const uint32_t bars = sbase + kOffBars;
+    // barrier map (8 bytes each)
     auto full_pk = [&](int s) { return bars + 8 * s; };
     auto empty_pk = [&](int s) { return bars + 8 * (kPkStages + s); };
     auto full_op = [&](int s) { return bars + 8 * (2 * kPkStages + s); };
-    auto empty_op = [&](int s) { return bars + 8 * (2 * kPkStages + kOpStages + s); };
-    const uint32_t acc_full = bars + 8 * (2 * kPkStages + 2 * kOpStages);
+    auto empty_pair = [&](int s) { return bars + 8 * (2 * kPkStages + kOpStages + s); };
+    const uint32_t acc_full = bars + 8 * (2 * kPkStages + kOpStages + 2);
     const uint32_t acc_empty = acc_full + 8;
     const uint32_t drain = acc_full + 16;
-    uint8_t *bar_ptr = smem + kOffBars;
-    volatile uint32_t *tmem_slot =
-        reinterpret_cast<volatile uint32_t *>(bar_ptr + 8 * (2 * kPkStages + 2 * kOpStages + 3));
+    volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(
+        smem + kOffBars + 8 * (2 * kPkStages + kOpStages + 5));
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -289,10 +288,9 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
             mbar_init(full_pk(s), 1);
             mbar_init(empty_pk(s), kUnpackThreads);
         }
-        for (int s = 0; s < kOpStages; s++) {
-            mbar_init(full_op(s), kUnpackThreads);
-            mbar_init(empty_op(s), 1);
-        }
+        for (int s = 0; s < kOpStages; s++) mbar_init(full_op(s), kUnpackThreads);
+        mbar_init(empty_pair(0), 1);
+        mbar_init(empty_pair(1), 1);
         mbar_init(acc_full, 1);
         mbar_init(acc_empty, kUnpackThreads);
         mbar_init(drain, 1);
@@ -317,7 +315,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
     if (warp == kProducerWarp) {
         // ------------------------------------------------------ TMA producer
         if (lane == 0) {
-            uint32_t g = 0;  // global stage counter
+            uint32_t g = 0;  // stage counter (32 samples per stage)
             bool ok = true;
             for (int u = first; u < nunits && ok; u += stride) {
                 const Unit U = P.units[u];
@@ -356,12 +354,14 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         __syncwarp();
     } else if (warp == kMmaWarp) {
         // ------------------------------------------------------ MMA issuer
+        // Stages are consumed in pairs (64 samples): four Re MMAs, then four
+        // Im MMAs, then one commit releasing both operand slots.  Runs of
+        // MMAs into one accumulator and few commits keep the tensor pipe full.
         if (lane == 0) {
-            uint32_t g = 0, acc_phase = 0;
+            uint32_t gp = 0, acc_phase = 0;  // pair counter
+            uint32_t ncommit[2] = {0, 0};
             bool ok = true;
             const bool b_signed = (MAP == MAP_EXACT);
-            // Descriptors of operand slot 0; slot s adds its byte offset >> 4
-            // to the start-address field (shared addresses stay < 256 KiB).
             const uint64_t dRe0 = sdesc(op_y, 1024, 1024), dRe1 = sdesc(op_y + 4096, 1024, 1024);
             const uint64_t dIm0 = sdesc(op_y + 8192, 1024, 1024);
             const uint64_t dIm1 = sdesc(op_y + 12288, 1024, 1024);
@@ -371,31 +371,40 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                 const int nx = (U.tyx >> 20) & 3;
                 const uint32_t idesc = idesc_i8(128 * nx, b_signed);
                 const int nst = (U.t1 - U.t0 + kStageSamples - 1) / kStageSamples;
-                const bool last_unit = (u + stride >= nunits);
+                const int npair = (nst + 1) / 2;
                 // the epilogue of the previous unit must have drained TMEM
                 if (!mbar_wait(acc_empty, acc_phase ^ 1, abort_flag)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                for (int it = 0; it < nst; it++, g++) {
-                    const int s = g % kOpStages;
-                    const uint32_t ph = (g / kOpStages) & 1;
-                    if (!mbar_wait(full_op(s), ph, abort_flag)) {
+                for (int ip = 0; ip < npair; ip++, gp++) {
+                    const int ps = gp & 1;
+                    const uint32_t ph = (gp >> 1) & 1;
+                    const int nin = (2 * ip + 1 < nst) ? 2 : 1;  // stages in this pair
+                    if (!mbar_wait(full_op(2 * ps), ph, abort_flag) ||
+                        !mbar_wait(full_op(2 * ps + 1), ph, abort_flag)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
-                    const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
-                    const uint32_t first_k = (it > 0) ? 1u : 0u;
-                    mma_i8(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, first_k);        // Re
-                    mma_i8(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, first_k);  // Im
-                    mma_i8(tmem_base, dRe1 + so_y, dX1 + so_x, idesc, 1u);             // Re
-                    mma_i8(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);       // Im
-                    // Release the operand slot unless nothing will refill it:
-                    // no arrival may be left pending when the CTA retires.
-                    if (!(last_unit && it + kOpStages >= nst)) mma_commit(empty_op(s));
+                    const uint32_t acc = (ip > 0) ? 1u : 0u;
+                    for (int j = 0; j < nin; j++) {
+                        const int s = 2 * ps + j;
+                        const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
+                        const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
+                        mma_i8(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, (j > 0) ? 1u : acc);
+                        mma_i8(tmem_base, dRe1 + so_y, dX1 + so_x, idesc, 1u);
+                    }
+                    for (int j = 0; j < nin; j++) {
+                        const int s = 2 * ps + j;
+                        const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
+                        const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
+                        mma_i8(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, (j > 0) ? 1u : acc);
+                        mma_i8(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);
+                    }
+                    mma_commit(empty_pair(ps));
+                    ncommit[ps]++;
                 }
                 if (!ok) break;
                 mma_commit(acc_full);
@@ -407,20 +416,25 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                 mma_commit(drain);
                 mbar_wait_drain(drain, 0);
             }
+            // No arrival may be pending when the CTA retires: wait for the
+            // last phase committed on each pair barrier.
+            for (int k = 0; k < 2; k++)
+                if (ncommit[k]) mbar_wait_drain(empty_pair(k), (ncommit[k] - 1) & 1);
         }
         __syncwarp();
     } else {
         // ------------------------------------------------------ unpack + epilogue
-        const int tid = threadIdx.x;  // 0..255
-        // y chunk: sample sy = tid >> 3, 16-element group gy = tid & 7
-        const int sy = tid >> 3, gy = tid & 7;
+        // Threads 0..255 convert the y tile (one 16-element chunk of one
+        // sample each), threads 256..511 the x tile (the same chunk position
+        // in each 128-element slice).
+        const int tid = threadIdx.x;  // 0..511
+        const bool is_y = tid < 256;
+        const int c = tid & 255;
+        const int sy = c >> 3, gy = c & 7;
         const uint32_t ry = (uint32_t)(sy & 7), by8 = (uint32_t)(sy >> 3);
-        const uint32_t ldy = (uint32_t)(sy * 128 + gy * 16);
-        const uint32_t sty_r = (2 * by8) * 1024 + swz(ry, gy);  // R; I at +1K
-        const uint32_t sty_i = 8192 + sty_r;                      // I; N at +1K
-        // x chunks c = tid + 256 j (slice j): the same sample and group as y
-        const uint32_t stx = (2 * by8) * 1024 + swz(ry, gy);
-        uint32_t g = 0, acc_phase = 0;
+        const uint32_t ldoff = (uint32_t)(sy * 128 + gy * 16);
+        const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);  // R (y) or X (x); I / Y at +1K
+        uint32_t g = 0, gp_base = 0, acc_phase = 0;
         bool ok = true;
         for (int u = first; u < nunits && ok; u += stride) {
             const Unit U = P.units[u];
@@ -435,54 +449,67 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                     break;
                 }
                 const bool valid = (U.t0 + it * kStageSamples + sy) < U.t1;
-                const uint4 wy = lds128(pk_y + ps * kPkYBytes + ldy);
-                const uint4 wx0 = lds128(pk_x + ps * kPkXBytes + ldy);
-                uint4 wx1 = make_uint4(0, 0, 0, 0);
-                if (nx > 1) wx1 = lds128(pk_x + ps * kPkXBytes + kPkYBytes + ldy);
-                // Convert before releasing the packed slot: the converted
-                // registers depend on the loaded words, so the slot is free
-                // once the arrive is visible.
-                uint32_t r[4], i[4], n[4], xr0[4], xi0[4], xr1[4], xi1[4];
-                yconv<MAP>(wy.x, r[0], i[0], n[0]);
-                yconv<MAP>(wy.y, r[1], i[1], n[1]);
-                yconv<MAP>(wy.z, r[2], i[2], n[2]);
-                yconv<MAP>(wy.w, r[3], i[3], n[3]);
-                xconv<MAP>(wx0.x, xr0[0], xi0[0]);
-                xconv<MAP>(wx0.y, xr0[1], xi0[1]);
-                xconv<MAP>(wx0.z, xr0[2], xi0[2]);
-                xconv<MAP>(wx0.w, xr0[3], xi0[3]);
-                xconv<MAP>(wx1.x, xr1[0], xi1[0]);
-                xconv<MAP>(wx1.y, xr1[1], xi1[1]);
-                xconv<MAP>(wx1.z, xr1[2], xi1[2]);
-                xconv<MAP>(wx1.w, xr1[3], xi1[3]);
+                uint32_t v0[4], v1[4], v2[4], v3[4];  // y: R, I, N; x: X0, Y0, X1, Y1
+                if (is_y) {
+                    const uint4 w = lds128(pk_y + ps * kPkYBytes + ldoff);
+                    yconv<MAP>(w.x, v0[0], v1[0], v2[0]);
+                    yconv<MAP>(w.y, v0[1], v1[1], v2[1]);
+                    yconv<MAP>(w.z, v0[2], v1[2], v2[2]);
+                    yconv<MAP>(w.w, v0[3], v1[3], v2[3]);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) v3[k] = 0u;
+                } else {
+                    const uint4 w0 = lds128(pk_x + ps * kPkXBytes + ldoff);
+                    uint4 w1 = make_uint4(0, 0, 0, 0);
+                    if (nx > 1) w1 = lds128(pk_x + ps * kPkXBytes + kPkYBytes + ldoff);
+                    xconv<MAP>(w0.x, v0[0], v1[0]);
+                    xconv<MAP>(w0.y, v0[1], v1[1]);
+                    xconv<MAP>(w0.z, v0[2], v1[2]);
+                    xconv<MAP>(w0.w, v0[3], v1[3]);
+                    xconv<MAP>(w1.x, v2[0], v3[0]);
+                    xconv<MAP>(w1.y, v2[1], v3[1]);
+                    xconv<MAP>(w1.z, v2[2], v3[2]);
+                    xconv<MAP>(w1.w, v2[3], v3[3]);
+                }
                 if (!valid) {  // samples outside the unit contribute zero
 #pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        r[k] = i[k] = n[k] = xr0[k] = xi0[k] = xr1[k] = xi1[k] = 0u;
+                    for (int k = 0; k < 4; k++) v0[k] = v1[k] = v2[k] = v3[k] = 0u;
                 }
+                // The converted registers depend on the loaded words: the
+                // packed slot is free once this arrive is visible.
                 mbar_arrive(empty_pk(ps));
 
-                const int os = g % kOpStages;
-                const uint32_t oph = (g / kOpStages) & 1;
-                if (!mbar_wait(empty_op(os), oph ^ 1, abort_flag)) {
+                // operand slot of stage `it`: pair (gp_base + it/2), half it&1
+                const uint32_t gpair = gp_base + (uint32_t)(it >> 1);
+                const int os = 2 * (int)(gpair & 1) + (it & 1);
+                if (!mbar_wait(empty_pair(gpair & 1), ((gpair >> 1) & 1) ^ 1, abort_flag)) {
                     ok = false;
                     break;
                 }
-                const uint32_t ya = op_y + os * kYOpBytes, xa = op_x + os * kXOpBytes;
-                sts128(ya + sty_r, r[0], r[1], r[2], r[3]);
-                sts128(ya + sty_r + 1024, i[0], i[1], i[2], i[3]);
-                sts128(ya + sty_i, i[0], i[1], i[2], i[3]);
-                sts128(ya + sty_i + 1024, n[0], n[1], n[2], n[3]);
-                sts128(xa + stx, xr0[0], xr0[1], xr0[2], xr0[3]);
-                sts128(xa + stx + 1024, xi0[0], xi0[1], xi0[2], xi0[3]);
-                if (nx > 1) {
-                    sts128(xa + 8192 + stx, xr1[0], xr1[1], xr1[2], xr1[3]);
-                    sts128(xa + 8192 + stx + 1024, xi1[0], xi1[1], xi1[2], xi1[3]);
+                // a pair cut short by an odd stage count still completes a
+                // phase on its second slot, keeping every slot's parity in step
+                const bool lone = (it == nst - 1) && ((it & 1) == 0);
+                if (is_y) {
+                    const uint32_t ya = op_y + os * kYOpBytes + st_a;
+                    sts128(ya, v0[0], v0[1], v0[2], v0[3]);                // R
+                    sts128(ya + 1024, v1[0], v1[1], v1[2], v1[3]);         // I
+                    sts128(ya + 8192, v1[0], v1[1], v1[2], v1[3]);         // I (Im copy)
+                    sts128(ya + 8192 + 1024, v2[0], v2[1], v2[2], v2[3]);  // N
+                } else {
+                    const uint32_t xa = op_x + os * kXOpBytes + st_a;
+                    sts128(xa, v0[0], v0[1], v0[2], v0[3]);  // X slice 0
+                    sts128(xa + 1024, v1[0], v1[1], v1[2], v1[3]);  // Y slice 0
+                    if (nx > 1) {
+                        sts128(xa + 8192, v2[0], v2[1], v2[2], v2[3]);  // X slice 1
+                        sts128(xa + 8192 + 1024, v3[0], v3[1], v3[2], v3[3]);  // Y slice 1
+                    }
                 }
                 fence_proxy_async();
                 mbar_arrive(full_op(os));
+                if (lone) mbar_arrive(full_op(os + 1));
             }
             if (!ok) break;
+            gp_base += (uint32_t)((nst + 1) / 2);
 
             // -------------------------------------------------- epilogue
             if (!mbar_wait(acc_full, acc_phase, abort_flag)) {
@@ -491,50 +518,54 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
             }
             acc_phase ^= 1;
             tc_fence_after();
-            const int q = warp & 3, h = warp >> 2;
+            const int q = warp & 3, h = warp >> 2;  // lane quarter, column group
             const int nb1 = cd->nb1;
             const int by = ty * 4 + q;
             int32_t *out = reinterpret_cast<int32_t *>(P.out_base + cd->out) + U.out_off;
             const int mode = U.split ? 2 : (P.accumulate ? 1 : 0);
-            const int nblk = 2 * nx;  // x blocks per warp
 #pragma unroll 1
-            for (int jj = 0; jj < nblk; jj++) {
-                const int j = h * nblk + jj;
-                uint32_t re[32], im[32];
-                const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + 32 * j;
-                tmem_ld32(taddr, re);
-                tmem_ld32(taddr + 256, im);
-                tmem_wait_ld();
+            for (int jj = 0; jj < nx; jj++) {
+                const int j = h * nx + jj;  // 32-column x block
                 const int bx = x0 * 4 + j;
-                if (by >= nb1 || bx >= nb1 || bx < by) continue;
+                const bool store = !(by >= nb1 || bx >= nb1 || bx < by);
                 const int64_t b = (int64_t)by * nb1 - (int64_t)by * (by - 1) / 2 + (bx - by);
                 int32_t *dst = out + (b * 32 + lane) * 64;
+                const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + 32 * j;
+#pragma unroll 1
+                for (int half = 0; half < 2; half++) {
+                    uint32_t re[16], im[16];
+                    tmem_ld16(taddr + 16 * half, re);
+                    tmem_ld16(taddr + 256 + 16 * half, im);
+                    tmem_wait_ld();
+                    if (!store) continue;
 #pragma unroll
-                for (int k = 0; k < 32; k++) {
-                    re[k] = (uint32_t)((int32_t)re[k] >> 4);
-                    im[k] = (uint32_t)((int32_t)im[k] >> 4);
-                    if (!P.ut) im[k] = 0u - im[k];
-                }
-                if (mode == 0) {
-#pragma unroll
-                    for (int k = 0; k < 32; k += 2)
-                        *reinterpret_cast<int4 *>(dst + 2 * k) =
-                            make_int4((int)re[k], (int)im[k], (int)re[k + 1], (int)im[k + 1]);
-                } else if (mode == 1) {
-#pragma unroll
-                    for (int k = 0; k < 32; k += 2) {
-                        int4 o = *reinterpret_cast<int4 *>(dst + 2 * k);
-                        o.x = (int)((uint32_t)o.x + re[k]);
-                        o.y = (int)((uint32_t)o.y + im[k]);
-                        o.z = (int)((uint32_t)o.z + re[k + 1]);
-                        o.w = (int)((uint32_t)o.w + im[k + 1]);
-                        *reinterpret_cast<int4 *>(dst + 2 * k) = o;
+                    for (int k = 0; k < 16; k++) {
+                        re[k] = (uint32_t)((int32_t)re[k] >> 4);
+                        im[k] = (uint32_t)((int32_t)im[k] >> 4);
+                        if (!P.ut) im[k] = 0u - im[k];
                     }
-                } else {
+                    int32_t *d = dst + 32 * half;
+                    if (mode == 0) {
 #pragma unroll
-                    for (int k = 0; k < 32; k++) {
-                        atomicAdd(dst + 2 * k, (int)re[k]);
-                        atomicAdd(dst + 2 * k + 1, (int)im[k]);
+                        for (int k = 0; k < 16; k += 2)
+                            *reinterpret_cast<int4 *>(d + 2 * k) =
+                                make_int4((int)re[k], (int)im[k], (int)re[k + 1], (int)im[k + 1]);
+                    } else if (mode == 1) {
+#pragma unroll
+                        for (int k = 0; k < 16; k += 2) {
+                            int4 o = *reinterpret_cast<int4 *>(d + 2 * k);
+                            o.x = (int)((uint32_t)o.x + re[k]);
+                            o.y = (int)((uint32_t)o.y + im[k]);
+                            o.z = (int)((uint32_t)o.z + re[k + 1]);
+                            o.w = (int)((uint32_t)o.w + im[k + 1]);
+                            *reinterpret_cast<int4 *>(d + 2 * k) = o;
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 16; k++) {
+                            atomicAdd(d + 2 * k, (int)re[k]);
+                            atomicAdd(d + 2 * k + 1, (int)im[k]);
+                        }
                     }
                 }
             }

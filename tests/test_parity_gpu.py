@@ -211,7 +211,8 @@ def test_full_size_overflow_edge_config(chimex, algo):
     _checksums(packed, blocks, T, F, E, seed=2, nspot=16)
 
 
-@pytest.mark.parametrize("E,F,T", [(2048, 16, 4096), (1024, 16, 15296), (2048, 32, 2048)])
+@pytest.mark.parametrize("E,F,T", [(2048, 16, 4096), (1024, 16, 15296), (2048, 32, 2048),
+                                   (2048, 4, 4000), (1536, 24, 1000)])
 def test_tc_repeatable_against_simt(chimex, E, F, T):
     """Persistent tensor-core launches over many units, repeated: every run
     must equal the CUDA-core kernel bit for bit (catches pipeline races that a
