@@ -590,12 +590,17 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
 
 template <int MAP>
 cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, cudaStream_t st) {
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(tc_correlate_kernel<MAP>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    // The shared-memory opt-in is a per-device function attribute.
+    static bool attr_done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr_done[dev]) {
+        e = cudaFuncSetAttribute(tc_correlate_kernel<MAP>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
         if (e != cudaSuccess) return e;
-        attr_done = true;
+        attr_done[dev] = true;
     }
     KParams P;
     P.chans = L.chans;
