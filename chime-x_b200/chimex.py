@@ -62,13 +62,14 @@ _sig("chx_corr_compat", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_blocks_to_triangle", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_blocks_to_full", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_plan_check", _i, [_vp, _vp])
+_sig("chx_correlate_noalloc", _i, [_vp, _vp, _i, _i, _i, _i, _i, _vp])
 
 EXPORTED = [
     "chx_version", "chx_last_error", "chx_plan_create", "chx_plan_destroy",
     "chx_plan_set_option", "chx_plan_block_words", "chx_plan_input_bytes",
     "chx_plan_sum_words", "chx_plan_triangle_words", "chx_correlate",
     "chx_offset_accumulate", "chx_preseed", "chx_corr_compat", "chx_blocks_to_triangle",
-    "chx_blocks_to_full", "chx_plan_check",
+    "chx_blocks_to_full", "chx_plan_check", "chx_correlate_noalloc",
 ]
 
 
@@ -100,6 +101,17 @@ def _stream(stream):
 def num_blocks(E):
     n = E // 32
     return n * (n + 1) // 2
+
+
+def correlate_noalloc(packed, blocks, E, F, T, upper_triangle_convention=1, accumulate=False,
+                      stream=None):
+    """chx_correlate_noalloc: the fused correlator without a plan and without
+    any allocation (for loops that must not allocate); `blocks` must already
+    hold F*NB*2048 int32."""
+    check(_lib.chx_correlate_noalloc(_ptr(packed), _ptr(blocks), E, F, T,
+                                     upper_triangle_convention, 1 if accumulate else 0,
+                                     _stream(stream)))
+    return blocks
 
 
 class Plan:

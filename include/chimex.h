@@ -138,6 +138,27 @@ int chx_blocks_to_triangle(chx_plan *plan, const int32_t *d_blocks,
 int chx_blocks_to_full(chx_plan *plan, const int32_t *d_blocks, int32_t *d_full,
                        void *stream);
 
+/* Fused correlator for callers that cannot allocate memory.  It has no
+ * counterpart in the reference.  It is meant for the per-frame loop of a
+ * real-time correlator that reserves all of its device memory at start-up:
+ * inside that loop cudaMalloc/cudaFree may stall every stream of the device
+ * (they can synchronise it), may fail once the reserved pools hold the
+ * memory, and are forbidden outright when another runtime owns the device
+ * allocator.  chx_correlate needs a plan, and creating a plan allocates.
+ * This entry point computes exactly what chx_correlate computes for a plan
+ * of (E, F, T, upper_triangle_convention), needs no plan and calls no
+ * allocator: its work tables live in a fixed-size array inside the library
+ * (about 140 KiB on every GPU that loads it, kept until exit).  Limits: F <= 64 channels and at
+ * most 4096 work units (72 per E=2048 channel per 262144 samples); larger
+ * calls return CHX_E_UNSUPPORTED.  The first call on each device looks the
+ * array up (and so loads the library's device code); make that first call
+ * before any stream capture.  All calls share the array: calls whose kernels
+ * overlap on the GPU race, so order them on one stream or with events.
+ * Device-side wait timeouts are not reported by this entry point. */
+int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks, int num_elements,
+                          int num_frequencies, int num_timesamples,
+                          int upper_triangle_convention, int accumulate, void *stream);
+
 /* Reads and clears the plan's device error word (bounded-wait timeouts).
  * Synchronises the stream.  Returns CHX_OK or CHX_E_TIMEOUT. */
 int chx_plan_check(chx_plan *plan, void *stream);
