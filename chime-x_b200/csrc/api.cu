@@ -3,6 +3,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+
 #include "chimex_internal.h"
 
 namespace chx {
@@ -53,19 +55,25 @@ cudaError_t build_tc_tables(chx_plan *p) {
     }
     std::vector<Unit> units;
     for (int f = 0; f < p->F; f++) tc_append_units(units, f, p->E, 0, p->T, p->tsplit, 0);
-    tc_sort_units(units);
+    const int grid = (int)std::min<size_t>(units.size(), (size_t)p->sm_count);
+    std::vector<int> offsets;
+    tc_schedule(units, grid, offsets);
     if (p->d_chans) cudaFree(p->d_chans);
     if (p->d_units) cudaFree(p->d_units);
     p->d_chans = p->d_units = nullptr;
+    const size_t ubytes = units.size() * sizeof(Unit);
     cudaError_t e = cudaMalloc(&p->d_chans, chans.size() * sizeof(ChanDesc));
-    if (e == cudaSuccess) e = cudaMalloc(&p->d_units, units.size() * sizeof(Unit));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_units, ubytes + offsets.size() * sizeof(int));
     if (e == cudaSuccess)
         e = cudaMemcpy(p->d_chans, chans.data(), chans.size() * sizeof(ChanDesc),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-        e = cudaMemcpy(p->d_units, units.data(), units.size() * sizeof(Unit),
+        e = cudaMemcpy(p->d_units, units.data(), ubytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy((char *)p->d_units + ubytes, offsets.data(), offsets.size() * sizeof(int),
                        cudaMemcpyHostToDevice);
     p->nunits = (int)units.size();
+    p->grid = grid;
     p->has_split_units = false;
     for (const Unit &u : units) p->has_split_units |= (u.split != 0);
     return e;
@@ -85,13 +93,14 @@ int run_tc(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, int map, int
     L.chans = (const ChanDesc *)p->d_chans;
     L.units = (const Unit *)p->d_units;
     L.nunits = p->nunits;
+    L.cta_offsets = (const int *)((const char *)p->d_units + (size_t)p->nunits * sizeof(Unit));
     L.out_base = (uint64_t)d_blocks;
     L.use_param_map = 1;
     L.map = map;
     L.ut = p->ut;
     L.accumulate = accumulate;
     L.err = p->d_err;
-    L.grid = p->nunits < p->sm_count ? p->nunits : p->sm_count;
+    L.grid = p->grid;
     CHX_CUDA(tc_launch(L, &tmap, st));
     return CHX_OK;
 }

@@ -43,8 +43,9 @@ struct chx_plan {
     int *d_err;   // device error word (bounded-wait timeouts)
     int sm_count;
     void *d_chans;  // tensor-core channel table (ChanDesc[F])
-    void *d_units;  // tensor-core work units (Unit[nunits])
+    void *d_units;  // tensor-core work units (Unit[nunits]) then grid + 1 offsets
     int nunits;
+    int grid;       // persistent CTAs of a tensor-core launch
     bool has_split_units;  // some output cells receive several units (atomic)
 };
 
@@ -126,8 +127,9 @@ constexpr int kUnitMaxSamples = 1 << 18;  // int32-exact bound per unit
 
 struct TcLaunch {
     const ChanDesc *chans;  // device
-    const Unit *units;      // device, sorted by decreasing cost
+    const Unit *units;      // device, grouped by CTA
     int nunits;
+    const int *cta_offsets; // device, grid + 1 entries
     uint64_t out_base;      // added to ChanDesc::out
     int use_param_map;      // 1: every channel uses the kernel-parameter map
     int map;                // value map (MAP_*)
@@ -141,7 +143,9 @@ bool tc_supported(int E, int T);
 // Appends the units of one channel's sample range [t_begin, t_end) to `out`.
 void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t_end,
                      int tsplit, long long out_off);
-void tc_sort_units(std::vector<Unit> &u);
+// Assigns units to `grid` persistent CTAs (longest first, to the least
+// loaded CTA) and reorders them CTA by CTA; offsets gets grid + 1 entries.
+void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets);
 // Encodes the TMA map of packed samples: dims {E, channels, samples}.
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
                   int64_t chan_stride, int64_t sample_stride);

@@ -35,7 +35,9 @@ constexpr int kNoAllocMaxUnits = 4096;
 constexpr size_t kOffErr = 0;
 constexpr size_t kOffChans = 256;
 constexpr size_t kOffUnits = kOffChans + sizeof(ChanDesc) * kNoAllocMaxChannels;
-constexpr size_t kScratchBytes = kOffUnits + sizeof(Unit) * kNoAllocMaxUnits;  // 140.25 KiB
+constexpr size_t kOffOffsets = kOffUnits + sizeof(Unit) * kNoAllocMaxUnits;
+constexpr int kNoAllocMaxGrid = 1024;
+constexpr size_t kScratchBytes = kOffOffsets + sizeof(int) * (kNoAllocMaxGrid + 1);  // ~144 KiB
 
 // The scratch: error word, channel table, unit table.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -43,8 +45,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void *g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch
-// Host staging for the tables (copied to the device every call).
+// Host staging for the tables (copied to the device every call) and for the
+// largest-first unit order before it is dealt to the CTAs.
 alignas(64) unsigned char g_host_tables[kScratchBytes];
+Unit g_host_sorted[kNoAllocMaxUnits];
 
 // Device address of the scratch array on the current device, looked up once
 // per device.  In host code the symbol itself is only a host-side stand-in.
@@ -112,7 +116,7 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
         chans[f].nb1 = E / 32;
         chans[f].fcoord = f;
     }
-    Unit *units = reinterpret_cast<Unit *>(g_host_tables + kOffUnits);
+    Unit *units = g_host_sorted;
     int n = 0;
     for (int f = 0; f < F; f++)
         for (int ty = 0; ty < nt; ty++)
@@ -128,8 +132,20 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
                     u.split = chunks > 1 ? 1 : 0;
                     u.cost = ((u.t1 - u.t0 + 31) / 32) * (nx + 1);
                 }
-    // Largest first, sorted in place (std::sort does not allocate).
+    // Largest first, sorted in place (std::sort does not allocate), then dealt
+    // round robin: CTA b takes sorted units b, b + grid, ... stored contiguously.
     std::sort(units, units + n, [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
+    int sm_count = 0;
+    CHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = std::min(std::min(n, sm_count), kNoAllocMaxGrid);
+    Unit *dealt = reinterpret_cast<Unit *>(g_host_tables + kOffUnits);
+    int *offsets = reinterpret_cast<int *>(g_host_tables + kOffOffsets);
+    int k = 0;
+    for (int b = 0; b < grid; b++) {
+        offsets[b] = k;
+        for (int i = b; i < n; i += grid) dealt[k++] = units[i];
+    }
+    offsets[grid] = k;
 
     cudaStream_t st = (cudaStream_t)stream;
     unsigned char *dscr = static_cast<unsigned char *>(scratch);
@@ -137,27 +153,28 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
     CHX_CUDA(cudaMemsetAsync(dscr + kOffErr, 0, sizeof(int), st));
     CHX_CUDA(cudaMemcpyAsync(dscr + kOffChans, chans, sizeof(ChanDesc) * F,
                              cudaMemcpyHostToDevice, st));
-    CHX_CUDA(cudaMemcpyAsync(dscr + kOffUnits, units, sizeof(Unit) * n, cudaMemcpyHostToDevice,
+    CHX_CUDA(cudaMemcpyAsync(dscr + kOffUnits, dealt, sizeof(Unit) * n, cudaMemcpyHostToDevice,
                              st));
+    CHX_CUDA(cudaMemcpyAsync(dscr + kOffOffsets, offsets, sizeof(int) * (grid + 1),
+                             cudaMemcpyHostToDevice, st));
     if (chunks > 1 && !accumulate)
         CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)F * nb * 2048 * 4, st));
 
     CUtensorMap tmap;
     const int r = tc_encode_map(&tmap, d_packed, E, F, T, E, (int64_t)F * E);
     if (r != 0) return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", r);
-    int sm_count = 0;
-    CHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
     TcLaunch L;
     L.chans = reinterpret_cast<const ChanDesc *>(dscr + kOffChans);
     L.units = reinterpret_cast<const Unit *>(dscr + kOffUnits);
     L.nunits = n;
+    L.cta_offsets = reinterpret_cast<const int *>(dscr + kOffOffsets);
     L.out_base = (uint64_t)d_blocks;
     L.use_param_map = 1;
     L.map = MAP_EXACT;
     L.ut = upper_triangle_convention;
     L.accumulate = accumulate ? 1 : 0;
     L.err = reinterpret_cast<int *>(dscr + kOffErr);
-    L.grid = n < sm_count ? n : sm_count;
+    L.grid = grid;
     CHX_CUDA(tc_launch(L, &tmap, st));
     return CHX_OK;
 }

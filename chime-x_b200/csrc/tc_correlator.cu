@@ -27,8 +27,8 @@
 //   Re += [R0 I0 R1 I1].[X0 Y0 X1 Y1]    Im += [I0 N0 I1 N1].[X0 Y0 X1 Y1]
 //   Re += [R2 I2 R3 I3].[X2 Y2 X3 Y3]    Im += [I2 N2 I3 N3].[X2 Y2 X3 Y3]
 //
-// Roles (576 threads, one persistent CTA per SM, units taken round-robin from
-// a table sorted by decreasing cost):
+// Roles (576 threads, one persistent CTA per SM; each CTA works through its
+// own contiguous range of the unit table, assigned on the host by cost):
 //   warps 0-15 unpack: read packed bytes from the TMA ring, convert with SWAR
 //              logic, store swizzled operand rows (warps 0-7 the y tile,
 //              8-15 the x tile); then the epilogue (TMEM -> block layout).
@@ -252,6 +252,7 @@ struct KParams {
     const ChanDesc *chans;
     const Unit *units;
     int nunits;
+    const int *cta_offsets;  // CTA b takes units [cta_offsets[b], cta_offsets[b+1])
     uint64_t out_base;
     int use_param_map;
     int ut;
@@ -309,15 +310,15 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int nunits = P.nunits;
-    const int first = blockIdx.x, stride = gridDim.x;
+    // This CTA's units: a contiguous range of the table, balanced on the host.
+    const int first = P.cta_offsets[blockIdx.x], last = P.cta_offsets[blockIdx.x + 1];
 
     if (warp == kProducerWarp) {
         // ------------------------------------------------------ TMA producer
         if (lane == 0) {
             uint32_t g = 0;  // stage counter (32 samples per stage)
             bool ok = true;
-            for (int u = first; u < nunits && ok; u += stride) {
+            for (int u = first; u < last && ok; u++) {
                 const Unit U = P.units[u];
                 const ChanDesc *cd = P.chans + U.chan;
                 const CUtensorMap *map = P.use_param_map ? &pmap : &cd->map;
@@ -366,7 +367,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
             const uint64_t dIm0 = sdesc(op_y + 8192, 1024, 1024);
             const uint64_t dIm1 = sdesc(op_y + 12288, 1024, 1024);
             const uint64_t dX0 = sdesc(op_x, 8192, 1024), dX1 = sdesc(op_x + 4096, 8192, 1024);
-            for (int u = first; u < nunits && ok; u += stride) {
+            for (int u = first; u < last && ok; u++) {
                 const Unit U = P.units[u];
                 const int nx = (U.tyx >> 20) & 3;
                 const uint32_t idesc = idesc_i8(128 * nx, b_signed);
@@ -436,7 +437,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);  // R (y) or X (x); I / Y at +1K
         uint32_t g = 0, gp_base = 0, acc_phase = 0;
         bool ok = true;
-        for (int u = first; u < nunits && ok; u += stride) {
+        for (int u = first; u < last && ok; u++) {
             const Unit U = P.units[u];
             const ChanDesc *cd = P.chans + U.chan;
             const int ty = U.tyx & 1023, x0 = (U.tyx >> 10) & 1023, nx = (U.tyx >> 20) & 3;
@@ -606,6 +607,7 @@ cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, cudaStream_t 
     P.chans = L.chans;
     P.units = L.units;
     P.nunits = L.nunits;
+    P.cta_offsets = L.cta_offsets;
     P.out_base = L.out_base;
     P.use_param_map = L.use_param_map;
     P.ut = L.ut;
@@ -642,16 +644,42 @@ void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t
                 u.t1 = std::min(t_end, u.t0 + chunk);
                 u.out_off = out_off;
                 u.split = splits > 1 ? 1 : 0;
-                u.cost = ((u.t1 - u.t0 + kStageSamples - 1) / kStageSamples) * (nx + 1);
+                u.cost = ((u.t1 - u.t0 + kStageSamples - 1) / kStageSamples) * (2 * nx + 1);
                 out.push_back(u);
             }
         }
     }
 }
 
-void tc_sort_units(std::vector<Unit> &u) {
+void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets) {
+    // Longest-processing-time-first: hand each unit, largest first, to the
+    // CTA with the least assigned cost, then store the units CTA by CTA.
     std::stable_sort(u.begin(), u.end(),
                      [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
+    if (grid < 1) grid = 1;
+    std::vector<long long> load(grid, 0);
+    std::vector<int> owner(u.size());
+    std::vector<std::pair<long long, int>> heap;  // (load, cta), min-heap
+    heap.reserve(grid);
+    for (int b = 0; b < grid; b++) heap.push_back({0, b});
+    auto cmp = [](const std::pair<long long, int> &a, const std::pair<long long, int> &b) {
+        return a.first != b.first ? a.first > b.first : a.second > b.second;
+    };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    for (size_t i = 0; i < u.size(); i++) {
+        std::pop_heap(heap.begin(), heap.end(), cmp);
+        auto &top = heap.back();
+        owner[i] = top.second;
+        top.first += u[i].cost;
+        std::push_heap(heap.begin(), heap.end(), cmp);
+    }
+    offsets.assign(grid + 1, 0);
+    for (size_t i = 0; i < u.size(); i++) offsets[owner[i] + 1]++;
+    for (int b = 0; b < grid; b++) offsets[b + 1] += offsets[b];
+    std::vector<int> fill(offsets.begin(), offsets.end() - 1);
+    std::vector<Unit> out(u.size());
+    for (size_t i = 0; i < u.size(); i++) out[fill[owner[i]]++] = u[i];
+    u.swap(out);
 }
 
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
