@@ -221,6 +221,8 @@ def run_plain(args, torch, cx, dist):
         plan.set_option(cx.OPT_ALGO, cx.ALGO_TC)
     if args.tsplit:
         plan.set_option(cx.OPT_TSPLIT, args.tsplit)
+    if args.tile:
+        plan.set_option(cx.OPT_TILE, args.tile)
     gen = torch.Generator(device=dev)
     gen.manual_seed(42 + rank)
     packed = torch.randint(0, 256, (plan.input_bytes,), dtype=torch.uint8, device=dev,
@@ -293,7 +295,7 @@ def run_plain(args, torch, cx, dist):
                 "device-generated",
         "config": {"workload": "plain correlator E=%d F=%d T=%d time_accum=256 per GPU, "
                                "one chx_correlate launch per step" % (E, F, T),
-                   "E": E, "F": F, "T": T, "time_accum": TA, "algo": args.algo,
+                   "E": E, "F": F, "T": T, "time_accum": TA, "algo": args.algo, "tile": args.tile,
                    "l2": "inputs (%d MiB) %s L2 (126 MB); no flush" % (
                        E * F * T >> 20, "larger than" if E * F * T > 126e6 else "SMALLER than"),
                    "parallelism": "channel shards, %d GPU(s), no collective" % world},
@@ -392,6 +394,7 @@ def main():
     ap.add_argument("--config", default="plain", choices=["plain", "batched", "stream"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "tc"])
     ap.add_argument("--tsplit", type=int, default=0)
+    ap.add_argument("--tile", type=int, default=0, help="tensor-core tile: 0 auto, 1 one SM, 2 SM pair")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

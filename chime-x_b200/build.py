@@ -50,7 +50,7 @@ def build(clean=False, verbose=False):
     if clean and os.path.isdir(OBJ):
         shutil.rmtree(OBJ)
     os.makedirs(OBJ, exist_ok=True)
-    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(ROOT, "include", "chimex.h"))
     sources = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
     jobs = []

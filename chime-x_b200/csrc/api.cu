@@ -54,8 +54,15 @@ cudaError_t build_tc_tables(chx_plan *p) {
         chans[f].fcoord = f;
     }
     std::vector<Unit> units;
-    for (int f = 0; f < p->F; f++) tc_append_units(units, f, p->E, 0, p->T, p->tsplit, 0);
-    const int grid = (int)std::min<size_t>(units.size(), (size_t)p->sm_count);
+    const int tile = p->tile ? p->tile : tc_default_tile(p->E);
+    for (int f = 0; f < p->F; f++) {
+        if (tile == kTile2Sm)
+            tc_append_pair_units(units, f, p->E, 0, p->T, p->tsplit, 0);
+        else
+            tc_append_units(units, f, p->E, 0, p->T, p->tsplit, 0);
+    }
+    const int slots = tile == kTile2Sm ? p->sm_count / 2 : p->sm_count;
+    const int grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, slots));
     std::vector<int> offsets;
     tc_schedule(units, grid, offsets);
     if (p->d_chans) cudaFree(p->d_chans);
@@ -74,6 +81,7 @@ cudaError_t build_tc_tables(chx_plan *p) {
                        cudaMemcpyHostToDevice);
     p->nunits = (int)units.size();
     p->grid = grid;
+    p->tile_built = tile;
     p->has_split_units = false;
     for (const Unit &u : units) p->has_split_units |= (u.split != 0);
     return e;
@@ -101,7 +109,10 @@ int run_tc(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, int map, int
     L.accumulate = accumulate;
     L.err = p->d_err;
     L.grid = p->grid;
-    CHX_CUDA(tc_launch(L, &tmap, st));
+    if (p->tile_built == kTile2Sm)
+        CHX_CUDA(tc_pair_launch(L, &tmap, st));
+    else
+        CHX_CUDA(tc_launch(L, &tmap, st));
     return CHX_OK;
 }
 
@@ -193,10 +204,15 @@ int chx_plan_set_option(chx_plan *p, int option, int64_t value) {
         CHX_CUDA(build_tc_tables(p));
         return CHX_OK;
     }
-    case CHX_OPT_TILE:
-        if (value < 0 || value > 16) return fail(CHX_E_INVALID, "tile %lld", (long long)value);
+    case CHX_OPT_TILE: {
+        if (value < 0 || value > kTile2Sm)
+            return fail(CHX_E_INVALID, "tile variant %lld (0 auto, 1 one SM, 2 SM pair)",
+                        (long long)value);
         p->tile = (int)value;
+        DeviceGuard g(p->device);
+        CHX_CUDA(build_tc_tables(p));
         return CHX_OK;
+    }
     default:
         return fail(CHX_E_INVALID, "unknown option %d", option);
     }

@@ -45,7 +45,8 @@ struct chx_plan {
     void *d_chans;  // tensor-core channel table (ChanDesc[F])
     void *d_units;  // tensor-core work units (Unit[nunits]) then grid + 1 offsets
     int nunits;
-    int grid;       // persistent CTAs of a tensor-core launch
+    int grid;       // persistent CTAs (or CTA pairs) of a tensor-core launch
+    int tile_built; // tile variant the tables were built for
     bool has_split_units;  // some output cells receive several units (atomic)
 };
 
@@ -150,5 +151,18 @@ void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets);
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
                   int64_t chan_stride, int64_t sample_stride);
 cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st);
+
+// ---- 2-SM tensor-core kernel (tc_pair_correlator.cu) ----
+// Units of 256 x 256 elements (tyx = ty2 | tx2 << 10, 128-element tile pairs),
+// computed by a cluster of two CTAs with tcgen05.mma.cta_group::2.  In the
+// launch, grid counts clusters and cta_offsets is indexed by cluster.
+void tc_append_pair_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t_end,
+                          int tsplit, long long out_off);
+cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st);
+
+// Tensor-core tile variants (CHX_OPT_TILE).
+constexpr int kTile1Sm = 1;  // 128 x 256 elements per CTA
+constexpr int kTile2Sm = 2;  // 256 x 256 elements per CTA pair
+int tc_default_tile(int E);
 
 }  // namespace chx

@@ -60,7 +60,8 @@ extern "C" {
 /* Plan options. */
 #define CHX_OPT_ALGO 1      /* one of CHX_ALGO_* */
 #define CHX_OPT_TSPLIT 2    /* number of sample-range splits (0 = auto) */
-#define CHX_OPT_TILE 3      /* tensor-core tile variant (0 = auto) */
+#define CHX_OPT_TILE 3      /* tensor-core tile variant: 0 auto, 1 one SM
+                               (128 x 256 elements), 2 SM pair (256 x 256) */
 
 typedef struct chx_plan chx_plan;
 

@@ -28,14 +28,21 @@ def chimex():
     return cx
 
 
-ALGOS = ["simt", "tc"]
+ALGOS = ["simt", "tc", "tc2"]  # tc: one-SM tile, tc2: SM-pair tile
 
 
-def make_plan(cx, E, F, T, TA=256, ut=1, kb=0, algo="auto", tsplit=0):
+def make_plan(cx, E, F, T, TA=256, ut=1, kb=0, algo="auto", tsplit=0, tile=0):
     p = cx.Plan(E, F, T, TA, ut, kb, 0)
+    if tile:
+        p.set_option(cx.OPT_TILE, tile)
     if algo == "simt":
         p.set_option(cx.OPT_ALGO, cx.ALGO_SIMT)
-    elif algo == "tc":
+    elif algo in ("tc", "tc2"):
+        if algo == "tc2":
+            tile = 2
+        elif not tile:
+            tile = 1
+        p.set_option(cx.OPT_TILE, tile)
         try:
             p.set_option(cx.OPT_ALGO, cx.ALGO_TC)
         except cx.ChimexError as e:
@@ -51,8 +58,8 @@ def to_dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def gpu_blocks(cx, packed, E, F, T, ut=1, algo="auto", tsplit=0):
-    p = make_plan(cx, E, F, T, ut=ut, algo=algo, tsplit=tsplit)
+def gpu_blocks(cx, packed, E, F, T, ut=1, algo="auto", tsplit=0, tile=0):
+    p = make_plan(cx, E, F, T, ut=ut, algo=algo, tsplit=tsplit, tile=tile)
     out = p.correlate(to_dev(packed))
     p.check_device()
     return out.cpu().numpy()
@@ -222,9 +229,10 @@ def test_tc_repeatable_against_simt(chimex, E, F, T):
     gen.manual_seed(E + F + T)
     d = torch.randint(0, 256, (T * F * E,), dtype=torch.uint8, device="cuda", generator=gen)
     ref = make_plan(chimex, E, F, T, algo="simt").correlate(d)
-    p = make_plan(chimex, E, F, T, algo="tc")
-    out = torch.empty_like(ref)
-    for _ in range(4):
-        p.correlate(d, out)
-        p.check_device()
-        assert torch.equal(out, ref)
+    for algo in ("tc", "tc2"):
+        p = make_plan(chimex, E, F, T, algo=algo)
+        out = torch.empty_like(ref)
+        for _ in range(4):
+            p.correlate(d, out)
+            p.check_device()
+            assert torch.equal(out, ref), algo
