@@ -64,12 +64,49 @@ _sig("chx_blocks_to_full", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_plan_check", _i, [_vp, _vp])
 _sig("chx_correlate_noalloc", _i, [_vp, _vp, _i, _i, _i, _i, _i, _vp])
 
+
+class ChannelDesc(ctypes.Structure):
+    """chx_channel_desc: one channel of a batch."""
+    _fields_ = [("num_elements", _i), ("num_timesamples", _i), ("num_integrations", _i),
+                ("input_stride", _i64), ("d_packed", _vp), ("d_blocks", _vp)]
+
+
+class StreamStats(ctypes.Structure):
+    """chx_stream_stats."""
+    _fields_ = [("frames", _i64), ("dumps", _i64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("resident_bytes", _i64)]
+
+
+_sig("chx_batch_create", _i, [ctypes.POINTER(_vp), _i, ctypes.POINTER(ChannelDesc), _i, _i])
+_sig("chx_batch_run", _i, [_vp, _vp, _i])
+_sig("chx_batch_work_units", _i64, [_vp])
+_sig("chx_batch_ops", ctypes.c_double, [_vp])
+_sig("chx_batch_check", _i, [_vp, _vp])
+_sig("chx_batch_destroy", _i, [_vp])
+_sig("chx_autotune", _i, [_i, _i, _vp, _vp, _vp, ctypes.POINTER(_i), ctypes.POINTER(_i),
+                          ctypes.POINTER(ctypes.c_double)])
+_sig("chx_stream_create", _i, [ctypes.POINTER(_vp), _i, _i, _i, _i64, _i])
+_sig("chx_stream_admit", _i, [_vp, _i, _i, ctypes.POINTER(_i)])
+_sig("chx_stream_frame_slot", _i, [_vp, _i, ctypes.POINTER(_vp)])
+_sig("chx_stream_submit", _i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_vp),
+                               ctypes.POINTER(_i64), _vp])
+_sig("chx_stream_last_dump", _i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_i64)])
+_sig("chx_stream_stats_get", _i, [_vp, ctypes.POINTER(StreamStats)])
+_sig("chx_stream_reset_stats", _i, [_vp])
+_sig("chx_stream_check", _i, [_vp])
+_sig("chx_stream_destroy", _i, [_vp])
+
 EXPORTED = [
     "chx_version", "chx_last_error", "chx_plan_create", "chx_plan_destroy",
     "chx_plan_set_option", "chx_plan_block_words", "chx_plan_input_bytes",
     "chx_plan_sum_words", "chx_plan_triangle_words", "chx_correlate",
     "chx_offset_accumulate", "chx_preseed", "chx_corr_compat", "chx_blocks_to_triangle",
     "chx_blocks_to_full", "chx_plan_check", "chx_correlate_noalloc",
+    "chx_batch_create", "chx_batch_run", "chx_batch_work_units", "chx_batch_ops",
+    "chx_batch_check", "chx_batch_destroy", "chx_autotune", "chx_stream_create",
+    "chx_stream_admit", "chx_stream_frame_slot", "chx_stream_submit", "chx_stream_last_dump",
+    "chx_stream_stats_get", "chx_stream_reset_stats", "chx_stream_check", "chx_stream_destroy",
 ]
 
 
@@ -96,6 +133,21 @@ def _stream(stream):
         import torch
         stream = torch.cuda.current_stream()
     return ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+class _DeviceArray:
+    """A raw device allocation seen through __cuda_array_interface__."""
+
+    def __init__(self, addr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (addr, False), "version": 3}
+
+
+def device_view(addr, n, dtype="int32", device=0):
+    """A torch tensor viewing n words at device address addr (no copy)."""
+    import torch
+    ts = {"int32": "<i4", "uint8": "|u1", "uint32": "<u4"}[dtype]
+    return torch.as_tensor(_DeviceArray(addr, n, ts), device=torch.device("cuda", device))
 
 
 def num_blocks(E):
@@ -230,3 +282,143 @@ class Plan:
 
     def check_device(self, stream=None):
         check(_lib.chx_plan_check(self._h, _stream(stream)))
+
+
+def autotune(E, T, scratch_in, scratch_out, stream=None):
+    """Times the tile variants and sample splits for (E, T) on the current
+    device (chx_autotune); returns (tile, split, ms) and caches the winner for
+    later batches."""
+    tile, split, ms = _i(), _i(), ctypes.c_double()
+    check(_lib.chx_autotune(E, T, _ptr(scratch_in), _ptr(scratch_out), _stream(stream),
+                            ctypes.byref(tile), ctypes.byref(split), ctypes.byref(ms)))
+    return tile.value, split.value, ms.value
+
+
+class Batch:
+    """Many channels (own E, integration length and count) in one persistent
+    launch captured in a CUDA graph (chx_batch_*).
+
+    channels: list of (packed, blocks, E, T, n_integrations[, input_stride]),
+    packed a uint8 CUDA tensor of n_integrations*T samples (stride bytes
+    apart, default E), blocks an int32 CUDA tensor of n_integrations*NB*2048.
+    The tensors must stay alive while the batch is used."""
+
+    def __init__(self, channels, upper_triangle_convention=1, device=0):
+        n = len(channels)
+        arr = (ChannelDesc * n)()
+        self._keep = []
+        for k, ch in enumerate(channels):
+            packed, blocks, E, T, nint = ch[:5]
+            stride = ch[5] if len(ch) > 5 else 0
+            if blocks.numel() < nint * num_blocks(E) * 2048:
+                raise ValueError("channel %d: blocks too small" % k)
+            if packed.numel() < ((nint * T - 1) * (stride or E) + E):
+                raise ValueError("channel %d: packed too small" % k)
+            arr[k] = ChannelDesc(E, T, nint, stride, packed.data_ptr(), blocks.data_ptr())
+            self._keep.append((packed, blocks))
+        self.device = device
+        h = ctypes.c_void_p()
+        check(_lib.chx_batch_create(ctypes.byref(h), n, arr, upper_triangle_convention, device))
+        self._h = h
+
+    def run(self, accumulate=False, stream=None):
+        check(_lib.chx_batch_run(self._h, _stream(stream), 1 if accumulate else 0))
+
+    @property
+    def work_units(self):
+        return _lib.chx_batch_work_units(self._h)
+
+    @property
+    def ops(self):
+        return _lib.chx_batch_ops(self._h)
+
+    def check_device(self, stream=None):
+        check(_lib.chx_batch_check(self._h, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.chx_batch_destroy(self._h)
+            self._h = None
+        self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Stream:
+    """Streaming correlation (chx_stream_*): frames of frame_len samples per
+    channel; each channel's integration of time_accum samples is correlated
+    and dumped as soon as its last frame is submitted."""
+
+    def __init__(self, max_channels, frame_len, upper_triangle_convention=1,
+                 hbm_budget_bytes=0, device=0):
+        h = ctypes.c_void_p()
+        check(_lib.chx_stream_create(ctypes.byref(h), max_channels, frame_len,
+                                     upper_triangle_convention, hbm_budget_bytes, device))
+        self._h = h
+        self.frame_len = frame_len
+        self.device = device
+        self.elements = []
+
+    def admit(self, E, time_accum):
+        cid = _i()
+        check(_lib.chx_stream_admit(self._h, E, time_accum, ctypes.byref(cid)))
+        self.elements.append(E)
+        return cid.value
+
+    def frame_slot(self, cid):
+        p = ctypes.c_void_p()
+        check(_lib.chx_stream_frame_slot(self._h, cid, ctypes.byref(p)))
+        return p.value
+
+    def submit(self, ids, frames=None, arrival_ns=None, stream=None):
+        """ids: channel ids (or a prepared ctypes int array); frames: None
+        (already in place) or a list of uint8 CUDA tensors / device addresses."""
+        n = len(ids)
+        ids_arr = ids if isinstance(ids, ctypes.Array) else (_i * n)(*ids)
+        fr = None
+        if frames is not None:
+            fr = (_vp * n)(*[f if isinstance(f, int) else f.data_ptr() for f in frames])
+        arr = None
+        if arrival_ns is not None:
+            arr = arrival_ns if isinstance(arrival_ns, ctypes.Array) else (_i64 * n)(*arrival_ns)
+        check(_lib.chx_stream_submit(self._h, n, ids_arr, fr, arr, _stream(stream)))
+
+    def last_dump(self, cid):
+        """(device address or None, sequence number) of the last completed dump."""
+        p, seq = ctypes.c_void_p(), _i64()
+        check(_lib.chx_stream_last_dump(self._h, cid, ctypes.byref(p), ctypes.byref(seq)))
+        return p.value, seq.value
+
+    def last_dump_tensor(self, cid):
+        """(int32 tensor view of the last completed dump, or None; sequence)."""
+        addr, seq = self.last_dump(cid)
+        if not addr:
+            return None, seq
+        return device_view(addr, num_blocks(self.elements[cid]) * 2048, "int32",
+                           self.device), seq
+
+    def stats(self):
+        st = StreamStats()
+        check(_lib.chx_stream_stats_get(self._h, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in StreamStats._fields_}
+
+    def reset_stats(self):
+        check(_lib.chx_stream_reset_stats(self._h))
+
+    def check_device(self):
+        check(_lib.chx_stream_check(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.chx_stream_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,427 @@
+// stream.cu -- streaming correlation: frames of samples arrive per channel,
+// integrations of time_accum samples are dumped as they complete.
+//
+// Memory per admitted channel (allocated at admission, resident until the
+// stream is destroyed): an input ring of two integrations (2 * TA * E bytes)
+// and two block buffers (2 * NB * 8 KiB), so one integration can be correlated
+// and read while the next fills.  A channel is admitted only when these fit
+// the HBM budget.
+//
+// Each submit appends one frame per listed channel to its ring (in place when
+// the caller wrote it into the slot returned by chx_stream_frame_slot).  The
+// channels whose integration completes are correlated by one persistent
+// tensor-core launch over all their work units: the integration's samples
+// accumulate in TMEM and each dump buffer is written once, so the resident
+// state never travels through HBM per frame.  A host callback after the launch
+// records, per integration, the latency from its last frame's arrival to the
+// completed dump.
+#include <time.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "chimex_internal.h"
+
+namespace chx {
+namespace {
+
+int64_t now_ns() {
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (int64_t)ts.tv_sec * 1000000000LL + ts.tv_nsec;
+}
+
+struct StreamChan {
+    int E = 0, TA = 0;
+    int64_t NB = 0;
+    uint8_t *ring = nullptr;     // [2][TA][E]
+    int32_t *dumps = nullptr;    // [2][NB][2048]
+    std::vector<Unit> units[2];  // work of ring half h -> dump h
+    int half = 0;                // half being filled
+    int filled = 0;              // samples in that half
+    int64_t seq = 0;             // integrations completed (dispatched)
+    int64_t last_arrival = 0;
+    // published by the completion callback
+    int64_t done_seq = -1;
+    int done_half = 0;
+};
+
+// One launch's unit table: pinned host staging, its device copy, and an event
+// recorded after the launch that reads it.
+struct Slot {
+    void *host = nullptr;
+    void *dev = nullptr;
+    cudaEvent_t done = nullptr;
+};
+constexpr int kSlots = 8;
+
+struct Pending {
+    struct Item {
+        int chan, half;
+        int64_t seq, arrival;
+    };
+    std::vector<Item> items;
+    struct chx_stream *owner;
+};
+
+}  // namespace
+}  // namespace chx
+
+using namespace chx;
+
+struct chx_stream {
+    int device = 0, max_channels = 0, frame_len = 0, ut = 1, tile = kTile2Sm, sm_count = 0;
+    int64_t budget = 0, resident = 0;
+    std::vector<StreamChan> chans;
+    ChanDesc *d_chans = nullptr;
+    std::vector<ChanDesc> h_chans;
+    Slot slots[kSlots];
+    size_t slot_cap = 0;  // bytes per slot: units + offsets
+    int next_slot = 0;
+    int *d_err = nullptr;
+    int64_t frames = 0, dumps = 0;
+    std::mutex mu;             // guards latencies and done_* fields
+    std::vector<double> latencies_ms;
+    std::vector<Pending *> inflight;
+};
+
+namespace {
+
+void CUDART_CB on_launch_done(void *arg) {
+    Pending *p = static_cast<Pending *>(arg);
+    const int64_t t = now_ns();
+    chx_stream *s = p->owner;
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (const auto &it : p->items) {
+        s->latencies_ms.push_back((double)(t - it.arrival) * 1e-6);
+        StreamChan &c = s->chans[it.chan];
+        if (it.seq > c.done_seq) {
+            c.done_seq = it.seq;
+            c.done_half = it.half;
+        }
+        s->dumps++;
+    }
+    p->items.clear();
+}
+
+void free_stream(chx_stream *s) {
+    for (auto &c : s->chans) {
+        if (c.ring) cudaFree(c.ring);
+        if (c.dumps) cudaFree(c.dumps);
+    }
+    if (s->d_chans) cudaFree(s->d_chans);
+    for (auto &sl : s->slots) {
+        if (sl.dev) cudaFree(sl.dev);
+        if (sl.host) cudaFreeHost(sl.host);
+        if (sl.done) cudaEventDestroy(sl.done);
+        sl = Slot();
+    }
+    if (s->d_err) cudaFree(s->d_err);
+    for (Pending *p : s->inflight) delete p;
+    s->inflight.clear();
+}
+
+}  // namespace
+
+extern "C" {
+
+int chx_stream_create(chx_stream **out, int max_channels, int frame_len, int ut, int64_t budget,
+                      int device) {
+    clear_error();
+    if (!out) return fail(CHX_E_INVALID, "NULL output");
+    *out = nullptr;
+    if (max_channels < 1 || max_channels > 65536)
+        return fail(CHX_E_INVALID, "max_channels=%d", max_channels);
+    if (frame_len < 1 || frame_len % 32) return fail(CHX_E_INVALID, "frame_len=%d must be a multiple of 32", frame_len);
+    if (ut != 0 && ut != 1) return fail(CHX_E_INVALID, "upper_triangle_convention=%d", ut);
+    int ndev = 0;
+    CHX_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(CHX_E_INVALID, "device=%d", device);
+    DeviceGuard g(device);
+    chx_stream *s = new (std::nothrow) chx_stream();
+    if (!s) return fail(CHX_E_NOMEM, "host allocation failed");
+    s->device = device;
+    s->max_channels = max_channels;
+    s->frame_len = frame_len;
+    s->ut = ut;
+    s->budget = budget;
+    s->chans.reserve(max_channels);
+    s->h_chans.resize(max_channels);
+    memset(s->h_chans.data(), 0, s->h_chans.size() * sizeof(ChanDesc));
+    cudaError_t e = cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_chans, (size_t)max_channels * sizeof(ChanDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->d_err, 0, sizeof(int));
+    for (int k = 0; k < kSlots && e == cudaSuccess; k++)
+        e = cudaEventCreateWithFlags(&s->slots[k].done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        free_stream(s);
+        delete s;
+        return cuda_fail(e, "stream set-up");
+    }
+    s->resident = (int64_t)max_channels * sizeof(ChanDesc);
+    *out = s;
+    return CHX_OK;
+}
+
+int chx_stream_admit(chx_stream *s, int E, int TA, int *channel_id) {
+    clear_error();
+    if (!s || !channel_id) return fail(CHX_E_INVALID, "NULL argument");
+    if ((int)s->chans.size() >= s->max_channels)
+        return fail(CHX_E_ADMISSION, "stream already holds %d channels", s->max_channels);
+    if (E < 32 || E % 32 || E > 65536) return fail(CHX_E_INVALID, "num_elements=%d", E);
+    if (TA < s->frame_len || TA % s->frame_len)
+        return fail(CHX_E_INVALID, "time_accum=%d must be a multiple of frame_len=%d", TA,
+                    s->frame_len);
+    if (TA > kUnitMaxSamples)
+        return fail(CHX_E_UNSUPPORTED, "time_accum=%d above %d samples", TA, kUnitMaxSamples);
+    DeviceGuard g(s->device);
+    const int64_t NB = num_blocks_of(E);
+    const int64_t ring_bytes = 2LL * TA * E;
+    const int64_t dump_bytes = 2LL * NB * 2048 * 4;
+    // units: both halves of this channel
+    std::vector<Unit> u0, u1;
+    const int cid = (int)s->chans.size();
+    tc_append_pair_units(u0, cid, E, 0, TA, 1, 0);
+    tc_append_pair_units(u1, cid, E, TA, 2 * TA, 1, NB * 2048);
+    const int64_t need = ring_bytes + dump_bytes;
+    if (s->budget > 0) {
+        if (s->resident + need > s->budget)
+            return fail(CHX_E_ADMISSION, "channel needs %lld bytes; %lld of %lld in use",
+                        (long long)need, (long long)s->resident, (long long)s->budget);
+    } else {
+        size_t fr = 0, tot = 0;
+        CHX_CUDA(cudaMemGetInfo(&fr, &tot));
+        const int64_t headroom = 2LL << 30;
+        if ((int64_t)fr < need + headroom)
+            return fail(CHX_E_ADMISSION, "channel needs %lld bytes; %lld free", (long long)need,
+                        (long long)fr);
+    }
+    StreamChan c;
+    c.E = E;
+    c.TA = TA;
+    c.NB = NB;
+    cudaError_t e = cudaMalloc(&c.ring, ring_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c.dumps, dump_bytes);
+    if (e == cudaSuccess) e = cudaMemset(c.dumps, 0, dump_bytes);
+    if (e != cudaSuccess) {
+        if (c.ring) cudaFree(c.ring);
+        if (c.dumps) cudaFree(c.dumps);
+        cudaGetLastError();
+        return fail(CHX_E_ADMISSION, "allocation for the channel failed: %s", cudaGetErrorString(e));
+    }
+    ChanDesc &d = s->h_chans[cid];
+    const int r = tc_encode_map(&d.map, c.ring, E, 1, 2LL * TA, E, E);
+    if (r != 0) {
+        cudaFree(c.ring);
+        cudaFree(c.dumps);
+        return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", r);
+    }
+    d.out = (uint64_t)c.dumps;
+    d.E = E;
+    d.nb1 = E / 32;
+    d.fcoord = 0;
+    CHX_CUDA(cudaMemcpy(s->d_chans + cid, &d, sizeof(ChanDesc), cudaMemcpyHostToDevice));
+    c.units[0] = std::move(u0);
+    c.units[1] = std::move(u1);
+    // Grow the per-launch unit tables to hold every channel completing at
+    // once.  Growing waits for all launches that read the old tables.
+    size_t total_units = c.units[0].size();
+    for (const auto &x : s->chans) total_units += x.units[0].size();
+    const size_t need_bytes = total_units * sizeof(Unit) + (size_t)(s->sm_count + 1) * sizeof(int);
+    if (need_bytes > s->slot_cap) {
+        const size_t cap = std::max(need_bytes, s->slot_cap * 2);
+        e = cudaDeviceSynchronize();
+        for (int k = 0; k < kSlots && e == cudaSuccess; k++) {
+            Slot &sl = s->slots[k];
+            if (sl.dev) cudaFree(sl.dev);
+            if (sl.host) cudaFreeHost(sl.host);
+            sl.dev = sl.host = nullptr;
+            e = cudaMalloc(&sl.dev, cap);
+            if (e == cudaSuccess) e = cudaMallocHost(&sl.host, cap);
+        }
+        if (e != cudaSuccess) {
+            cudaFree(c.ring);
+            cudaFree(c.dumps);
+            s->slot_cap = 0;  // the next admission reallocates every slot
+            return cuda_fail(e, "unit table growth");
+        }
+        s->slot_cap = cap;
+    }
+    s->resident += need;
+    s->chans.push_back(std::move(c));
+    *channel_id = cid;
+    return CHX_OK;
+}
+
+int chx_stream_frame_slot(chx_stream *s, int channel_id, uint8_t **d_slot) {
+    clear_error();
+    if (!s || !d_slot || channel_id < 0 || channel_id >= (int)s->chans.size())
+        return fail(CHX_E_INVALID, "bad channel");
+    StreamChan &c = s->chans[channel_id];
+    *d_slot = c.ring + ((int64_t)c.half * c.TA + c.filled) * c.E;
+    return CHX_OK;
+}
+
+int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const *d_frames,
+                      const int64_t *arrival_ns, void *stream) {
+    clear_error();
+    if (!s || (n > 0 && !ids)) return fail(CHX_E_INVALID, "NULL argument");
+    DeviceGuard g(s->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    Pending *pend = new (std::nothrow) Pending();
+    if (!pend) return fail(CHX_E_NOMEM, "host allocation failed");
+    pend->owner = s;
+    std::vector<Unit> units;
+    for (int i = 0; i < n; i++) {
+        const int id = ids[i];
+        if (id < 0 || id >= (int)s->chans.size()) {
+            delete pend;
+            return fail(CHX_E_INVALID, "channel id %d", id);
+        }
+        StreamChan &c = s->chans[id];
+        uint8_t *slot = c.ring + ((int64_t)c.half * c.TA + c.filled) * c.E;
+        const uint8_t *src = d_frames ? d_frames[i] : nullptr;
+        if (src && src != slot) {
+            const cudaError_t e = cudaMemcpyAsync(slot, src, (size_t)s->frame_len * c.E,
+                                                  cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) {
+                delete pend;
+                return cuda_fail(e, "frame copy");
+            }
+        }
+        c.filled += s->frame_len;
+        c.last_arrival = arrival_ns ? arrival_ns[i] : now_ns();
+        s->frames++;
+        if (c.filled == c.TA) {
+            units.insert(units.end(), c.units[c.half].begin(), c.units[c.half].end());
+            pend->items.push_back({id, c.half, c.seq, c.last_arrival});
+            c.seq++;
+            c.half ^= 1;
+            c.filled = 0;
+        }
+    }
+    if (units.empty()) {
+        delete pend;
+        return CHX_OK;
+    }
+    const int slots = std::max(1, s->sm_count / 2);
+    const int grid = (int)std::min<size_t>(units.size(), (size_t)slots);
+    std::vector<int> offsets;
+    tc_schedule(units, grid, offsets);
+    const size_t ub = units.size() * sizeof(Unit);
+    const size_t tb = ub + offsets.size() * sizeof(int);
+    if (tb > s->slot_cap) {
+        delete pend;
+        return fail(CHX_E_INVALID, "unit table overflow");
+    }
+    // Reuse the oldest slot once the launch that read it has finished.
+    Slot &sl = s->slots[s->next_slot];
+    s->next_slot = (s->next_slot + 1) % kSlots;
+    CHX_CUDA(cudaEventSynchronize(sl.done));
+    memcpy(sl.host, units.data(), ub);
+    memcpy((char *)sl.host + ub, offsets.data(), offsets.size() * sizeof(int));
+    CHX_CUDA(cudaMemcpyAsync(sl.dev, sl.host, tb, cudaMemcpyHostToDevice, st));
+    TcLaunch L;
+    L.chans = s->d_chans;
+    L.units = (const Unit *)sl.dev;
+    L.nunits = (int)units.size();
+    L.cta_offsets = (const int *)((const char *)sl.dev + ub);
+    L.out_base = 0;
+    L.use_param_map = 0;
+    L.map = MAP_EXACT;
+    L.ut = s->ut;
+    L.accumulate = 0;
+    L.err = s->d_err;
+    L.grid = grid;
+    CHX_CUDA(tc_pair_launch(L, nullptr, st));
+    CHX_CUDA(cudaEventRecord(sl.done, st));
+    CHX_CUDA(cudaLaunchHostFunc(st, on_launch_done, pend));
+    s->inflight.push_back(pend);
+    if (s->inflight.size() > 64) {  // reclaim records whose callback has run
+        std::lock_guard<std::mutex> lock(s->mu);
+        std::vector<Pending *> keep;
+        for (Pending *p : s->inflight) {
+            if (p->items.empty() && p != pend)
+                delete p;
+            else
+                keep.push_back(p);
+        }
+        s->inflight.swap(keep);
+    }
+    return CHX_OK;
+}
+
+int chx_stream_last_dump(chx_stream *s, int channel_id, const int32_t **d_blocks, int64_t *seq) {
+    clear_error();
+    if (!s || channel_id < 0 || channel_id >= (int)s->chans.size())
+        return fail(CHX_E_INVALID, "bad channel");
+    std::lock_guard<std::mutex> lock(s->mu);
+    const StreamChan &c = s->chans[channel_id];
+    if (c.done_seq < 0) {
+        if (d_blocks) *d_blocks = nullptr;
+        if (seq) *seq = -1;
+        return CHX_OK;
+    }
+    if (d_blocks) *d_blocks = c.dumps + (size_t)c.done_half * c.NB * 2048;
+    if (seq) *seq = c.done_seq;
+    return CHX_OK;
+}
+
+int chx_stream_stats_get(chx_stream *s, chx_stream_stats *out) {
+    clear_error();
+    if (!s || !out) return fail(CHX_E_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(s->mu);
+    out->frames = s->frames;
+    out->dumps = s->dumps;
+    out->resident_bytes = s->resident;
+    std::vector<double> v = s->latencies_ms;
+    if (v.empty()) {
+        out->p50_ms = out->p99_ms = out->max_ms = 0.0;
+        return CHX_OK;
+    }
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) {
+        const size_t k = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+        return v[k];
+    };
+    out->p50_ms = pct(0.50);
+    out->p99_ms = pct(0.99);
+    out->max_ms = v.back();
+    return CHX_OK;
+}
+
+int chx_stream_reset_stats(chx_stream *s) {
+    clear_error();
+    if (!s) return fail(CHX_E_INVALID, "NULL stream");
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->latencies_ms.clear();
+    return CHX_OK;
+}
+
+int chx_stream_check(chx_stream *s) {
+    clear_error();
+    if (!s) return fail(CHX_E_INVALID, "NULL stream");
+    DeviceGuard g(s->device);
+    CHX_CUDA(cudaDeviceSynchronize());
+    int h = 0;
+    CHX_CUDA(cudaMemcpy(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        CHX_CUDA(cudaMemset(s->d_err, 0, sizeof(int)));
+        return fail(CHX_E_TIMEOUT, "a bounded device wait gave up (code 0x%x)", h);
+    }
+    return CHX_OK;
+}
+
+int chx_stream_destroy(chx_stream *s) {
+    clear_error();
+    if (!s) return CHX_OK;
+    DeviceGuard g(s->device);
+    cudaDeviceSynchronize();
+    free_stream(s);
+    delete s;
+    return CHX_OK;
+}
+
+}  // extern "C"

@@ -189,6 +189,9 @@ int chx_batch_run(chx_batch *batch, void *stream, int accumulate);
 /* Work units (tile pairs x splits) in the queue, and exact ops per run. */
 int64_t chx_batch_work_units(const chx_batch *batch);
 double chx_batch_ops(const chx_batch *batch);
+/* Reads and clears the batch's device error word (bounded-wait timeouts).
+ * Synchronises the stream.  Returns CHX_OK or CHX_E_TIMEOUT. */
+int chx_batch_check(chx_batch *batch, void *stream);
 int chx_batch_destroy(chx_batch *batch);
 
 /* Times the tensor-core tile variants and split counts for (E, T) on the
@@ -199,41 +202,64 @@ int chx_autotune(int num_elements, int num_timesamples, const uint8_t *d_scratch
                  int *best_split, double *best_ms);
 
 /* ---------------------------------------------------------------------
- * Streaming: frames of samples arrive per channel; accumulators stay
- * resident in HBM and are dumped every time_accum samples.
+ * Streaming: frames of samples arrive per channel and every time_accum
+ * samples the channel's integration is correlated and dumped.  The reference
+ * has no streaming layer: its host loop (main_wrapper.c) correlates whole
+ * buffers; this is the serving form of the same correlation.
+ *
+ * Each admitted channel holds, until chx_stream_destroy, an input ring of two
+ * integrations (2*time_accum*E bytes) and two dump buffers (2*NB*8 KiB), all
+ * in HBM.  A submit appends one frame per listed channel; the channels whose
+ * integration completes are correlated by one tensor-core launch on the given
+ * stream (the integration accumulates in tensor memory and is written to its
+ * dump buffer once).
  * ------------------------------------------------------------------- */
 typedef struct chx_stream chx_stream;
 
 typedef struct chx_stream_stats {
-    int64_t frames;         /* frames correlated */
-    int64_t dumps;          /* integrations completed */
-    double p50_ms, p99_ms;  /* frame-to-visibility latency percentiles */
+    int64_t frames;         /* frames submitted */
+    int64_t dumps;          /* integrations completed on the device */
+    double p50_ms, p99_ms;  /* last-frame-arrival to dump-complete latency */
     double max_ms;
-    int64_t resident_bytes; /* HBM held by accumulators and dump buffers */
+    int64_t resident_bytes; /* HBM held by rings, dump buffers, channel table */
 } chx_stream_stats;
 
-/* hbm_budget_bytes = 0: admit while cudaMemGetInfo leaves headroom. */
+/* frame_len: samples per frame (multiple of 32).  hbm_budget_bytes > 0 caps
+ * the resident bytes; 0 admits while cudaMemGetInfo leaves 2 GiB free. */
 int chx_stream_create(chx_stream **s, int max_channels, int frame_len,
                       int upper_triangle_convention, int64_t hbm_budget_bytes,
                       int device);
-/* Admits a channel with E elements dumping every time_accum samples
- * (a multiple of frame_len).  Returns CHX_E_ADMISSION when its resident
- * accumulators (double buffered) do not fit the budget. */
+/* Admits a channel with E elements dumping every time_accum samples (a
+ * multiple of frame_len, at most 262144).  Returns CHX_E_ADMISSION, admitting
+ * nothing, when its ring and dump buffers do not fit. */
 int chx_stream_admit(chx_stream *s, int num_elements, int time_accum,
                      int *channel_id);
-/* Correlates one frame per listed channel (d_frames[i]: frame_len*E_c bytes
- * on the device) in one launch; arrival_ns are the frames' host arrival
- * times used for latency.  Completed integrations are swapped into the dump
- * buffers. */
+/* Device address where channel c's next frame (frame_len*E bytes) belongs.
+ * A producer that writes frames there itself (then submits with d_frames
+ * NULL) must not write into a ring half whose integration is still being
+ * correlated: wait for the dump of that integration first. */
+int chx_stream_frame_slot(chx_stream *s, int channel_id, uint8_t **d_slot);
+/* Appends one frame per listed channel.  d_frames NULL, or an entry equal to
+ * the channel's frame slot: the frame is already in place; otherwise
+ * d_frames[i] (device memory) is copied into the ring on `stream`.
+ * arrival_ns: CLOCK_MONOTONIC arrival time of each frame (NULL = now).  Host
+ * tables are reused after 8 launches, so a submit may wait for the launch
+ * 8 submits back. */
 int chx_stream_submit(chx_stream *s, int n, const int *channel_ids,
                       const uint8_t *const *d_frames, const int64_t *arrival_ns,
                       void *stream);
-/* Device pointer of channel c's last completed integration (NULL if none),
- * and its sequence number. */
+/* Channel c's last integration whose dump has completed on the device (NULL,
+ * seq -1 if none) and its sequence number.  The buffer is overwritten when
+ * integration seq+2 completes. */
 int chx_stream_last_dump(chx_stream *s, int channel_id, const int32_t **d_blocks,
                          int64_t *seq);
-/* Collects finished dump events and fills latency statistics. */
+/* Counters and latency percentiles over the dumps completed so far. */
 int chx_stream_stats_get(chx_stream *s, chx_stream_stats *out);
+/* Forgets the latency samples (counters stay). */
+int chx_stream_reset_stats(chx_stream *s);
+/* Synchronises the device, reads and clears the device error word.  Returns
+ * CHX_OK or CHX_E_TIMEOUT. */
+int chx_stream_check(chx_stream *s);
 int chx_stream_destroy(chx_stream *s);
 
 #ifdef __cplusplus
