@@ -200,6 +200,7 @@ def run_stream(args, torch, cx, dist):
     ticks = max(8 * per, (args.steps // per) * per)
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
+    s.sync()
     launches0 = s.stats()["dumps"]
     with B.ClockSampler(local_rank) as clk:
         clk.mark_start()

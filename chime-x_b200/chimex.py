@@ -95,6 +95,7 @@ _sig("chx_stream_last_dump", _i, [_vp, _i, ctypes.POINTER(_vp), ctypes.POINTER(_
 _sig("chx_stream_stats_get", _i, [_vp, ctypes.POINTER(StreamStats)])
 _sig("chx_stream_reset_stats", _i, [_vp])
 _sig("chx_stream_check", _i, [_vp])
+_sig("chx_stream_sync", _i, [_vp])
 _sig("chx_stream_destroy", _i, [_vp])
 
 EXPORTED = [
@@ -106,7 +107,8 @@ EXPORTED = [
     "chx_batch_create", "chx_batch_run", "chx_batch_work_units", "chx_batch_ops",
     "chx_batch_check", "chx_batch_destroy", "chx_autotune", "chx_stream_create",
     "chx_stream_admit", "chx_stream_frame_slot", "chx_stream_submit", "chx_stream_last_dump",
-    "chx_stream_stats_get", "chx_stream_reset_stats", "chx_stream_check", "chx_stream_destroy",
+    "chx_stream_stats_get", "chx_stream_reset_stats", "chx_stream_check", "chx_stream_sync",
+    "chx_stream_destroy",
 ]
 
 
@@ -408,6 +410,10 @@ class Stream:
 
     def reset_stats(self):
         check(_lib.chx_stream_reset_stats(self._h))
+
+    def sync(self):
+        """Waits until every submitted launch is complete and published."""
+        check(_lib.chx_stream_sync(self._h))
 
     def check_device(self):
         check(_lib.chx_stream_check(self._h))

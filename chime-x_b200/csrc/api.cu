@@ -52,6 +52,7 @@ cudaError_t build_tc_tables(chx_plan *p) {
         chans[f].E = p->E;
         chans[f].nb1 = (int)p->NB1;
         chans[f].fcoord = f;
+        chans[f].orow = (int)((int64_t)f * p->NB * 32);
     }
     std::vector<Unit> units;
     const int tile = p->tile ? p->tile : tc_default_tile(p->E);
@@ -87,14 +88,23 @@ cudaError_t build_tc_tables(chx_plan *p) {
     return e;
 }
 
+// The tensor-core path addresses the plan's blocks as F*NB*32 rows of a TMA map.
+bool plan_tc_ok(const chx_plan *p) {
+    return tc_supported(p->E, p->T) && tc_out_rows_ok((int64_t)p->F * p->NB * 32);
+}
+
 // Launches the tensor-core kernel on the plan's tables with `map`.
 int run_tc(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, int map, int accumulate,
            cudaStream_t st) {
     if ((reinterpret_cast<uintptr_t>(d_packed) & 15) != 0)
         return fail(CHX_E_INVALID, "packed input must be 16-byte aligned for TMA");
-    CUtensorMap tmap;
-    const int r = tc_encode_map(&tmap, d_packed, p->E, p->F, p->T, p->E, (int64_t)p->F * p->E);
+    if ((reinterpret_cast<uintptr_t>(d_blocks) & 15) != 0)
+        return fail(CHX_E_INVALID, "block buffer must be 16-byte aligned for TMA");
+    CUtensorMap tmap, omap;
+    int r = tc_encode_map(&tmap, d_packed, p->E, p->F, p->T, p->E, (int64_t)p->F * p->E);
     if (r != 0) return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", r);
+    r = tc_encode_out_map(&omap, d_blocks, (int64_t)p->F * p->NB * 32);
+    if (r != 0) return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled (blocks) failed (%d)", r);
     if (p->has_split_units && !accumulate)
         CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)chx_plan_block_words(p) * 4, st));
     TcLaunch L;
@@ -110,9 +120,9 @@ int run_tc(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, int map, int
     L.err = p->d_err;
     L.grid = p->grid;
     if (p->tile_built == kTile2Sm)
-        CHX_CUDA(tc_pair_launch(L, &tmap, st));
+        CHX_CUDA(tc_pair_launch(L, &tmap, &omap, st));
     else
-        CHX_CUDA(tc_launch(L, &tmap, st));
+        CHX_CUDA(tc_launch(L, &tmap, &omap, st));
     return CHX_OK;
 }
 
@@ -193,7 +203,7 @@ int chx_plan_set_option(chx_plan *p, int option, int64_t value) {
     case CHX_OPT_ALGO:
         if (value < CHX_ALGO_AUTO || value > CHX_ALGO_TC)
             return fail(CHX_E_INVALID, "unknown algorithm %lld", (long long)value);
-        if (value == CHX_ALGO_TC && !tc_supported(p->E, p->T))
+        if (value == CHX_ALGO_TC && !plan_tc_ok(p))
             return fail(CHX_E_UNSUPPORTED, "tensor-core path does not take E=%d T=%d", p->E, p->T);
         p->algo = (int)value;
         return CHX_OK;
@@ -243,7 +253,7 @@ int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void 
     DeviceGuard g(p->device);
     cudaStream_t st = (cudaStream_t)stream;
     const bool use_tc =
-        (p->algo == CHX_ALGO_TC) || (p->algo == CHX_ALGO_AUTO && tc_supported(p->E, p->T));
+        (p->algo == CHX_ALGO_TC) || (p->algo == CHX_ALGO_AUTO && plan_tc_ok(p));
     if (use_tc) return run_tc(p, d_packed, d_blocks, MAP_EXACT, accumulate ? 1 : 0, st);
     const int splits =
         p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);
@@ -301,7 +311,7 @@ int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, voi
     DeviceGuard g(p->device);
     cudaStream_t st = (cudaStream_t)stream;
     const int map = p->kernel_batch == CHX_KERNEL_PACKED ? MAP_PACKED : MAP_CONF;
-    if (p->algo != CHX_ALGO_SIMT && tc_supported(p->E, p->T))
+    if (p->algo != CHX_ALGO_SIMT && plan_tc_ok(p))
         return run_tc(p, d_packed, d_blocks, map, 1, st);
     const int splits =
         p->tsplit ? p->tsplit : auto_splits((int64_t)p->NB * p->F, p->T, p->sm_count, 256);

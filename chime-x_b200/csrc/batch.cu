@@ -105,9 +105,9 @@ int record_batch(chx_batch *b, cudaStream_t st, int accumulate) {
     L.err = b->d_err;
     L.grid = b->grid;
     if (b->tile == kTile2Sm)
-        CHX_CUDA(tc_pair_launch(L, nullptr, st));
+        CHX_CUDA(tc_pair_launch(L, nullptr, nullptr, st));
     else
-        CHX_CUDA(tc_launch(L, nullptr, st));
+        CHX_CUDA(tc_launch(L, nullptr, nullptr, st));
     return CHX_OK;
 }
 
@@ -130,6 +130,10 @@ int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int 
         if ((int64_t)d.num_timesamples * d.num_integrations > 2147483647LL)
             return fail(CHX_E_INVALID, "channel %d: too many samples", c);
         if (!d.d_packed || !d.d_blocks) return fail(CHX_E_INVALID, "channel %d: NULL buffer", c);
+        if (reinterpret_cast<uintptr_t>(d.d_blocks) & 15)
+            return fail(CHX_E_INVALID, "channel %d: block buffer must be 16-byte aligned", c);
+        if (!tc_out_rows_ok((int64_t)d.num_integrations * num_blocks_of(d.num_elements) * 32))
+            return fail(CHX_E_UNSUPPORTED, "channel %d: block buffers too large", c);
         const int64_t stride = d.input_stride ? d.input_stride : d.num_elements;
         if (stride < d.num_elements || stride % 16 || (reinterpret_cast<uintptr_t>(d.d_packed) & 15))
             return fail(CHX_E_INVALID,
@@ -186,6 +190,13 @@ int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int 
             delete b;
             return fail(CHX_E_CUDA, "channel %d: cuTensorMapEncodeTiled failed (%d)", c, r);
         }
+        const int64_t nb_c = num_blocks_of(d.num_elements);
+        const int r2 = tc_encode_out_map(&chans[c].omap, d.d_blocks, d.num_integrations * nb_c * 32);
+        if (r2 != 0) {
+            delete b;
+            return fail(CHX_E_CUDA, "channel %d: cuTensorMapEncodeTiled (blocks) failed (%d)", c, r2);
+        }
+        chans[c].orow = 0;
         chans[c].out = (uint64_t)d.d_blocks;
         chans[c].E = d.num_elements;
         chans[c].nb1 = d.num_elements / 32;

@@ -102,15 +102,17 @@ cudaError_t launch_blocks_to_full(const int32_t *blocks, int32_t *full, int E, i
 // A channel as the tensor-core kernel sees it: the TMA map of its packed
 // samples (dims {E, channels, samples}), its block-buffer address and shape.
 struct __align__(64) ChanDesc {
-    CUtensorMap map;  // used unless the launch passes one map for all channels
-    uint64_t out;     // block buffer: absolute address, or byte offset added to
-                      // the launch's out_base
-    int E;            // elements
-    int nb1;          // E / 32
-    int fcoord;       // channel coordinate inside the TMA map
-    int pad[11];
+    CUtensorMap map;   // samples; used unless the launch passes one map for all channels
+    CUtensorMap omap;  // block output as rows of 64 words (tc_encode_out_map); same rule
+    uint64_t out;      // block buffer: absolute address, or byte offset added to
+                       // the launch's out_base
+    int E;             // elements
+    int nb1;           // E / 32
+    int fcoord;        // channel coordinate inside the TMA map
+    int orow;          // first row of this channel's blocks inside omap
+    int pad[10];
 };
-static_assert(sizeof(ChanDesc) == 192, "ChanDesc layout");
+static_assert(sizeof(ChanDesc) == 320, "ChanDesc layout");
 
 // One work unit: a 128-element y tile against one or two 128-element x tiles
 // of one channel over samples [t0, t1).  tyx = ty | x0 << 10 | nx << 20.
@@ -150,7 +152,15 @@ void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets);
 // Encodes the TMA map of packed samples: dims {E, channels, samples}.
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
                   int64_t chan_stride, int64_t sample_stride);
-cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st);
+// Encodes the TMA map of a block buffer seen as `rows` rows of 64 int32 words
+// (one 32-cell block row of Re/Im pairs), tile {32 words, 32 rows}, 128-byte
+// swizzle.  The epilogues store (or add) their tiles through it.  rows must
+// stay below 2^31 (tc_out_rows_ok).
+int tc_encode_out_map(CUtensorMap *m, void *base, int64_t rows);
+inline bool tc_out_rows_ok(int64_t rows) { return rows > 0 && rows < (1LL << 31); }
+// param_map / param_omap: the maps every channel uses when L.use_param_map.
+cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map,
+                      const CUtensorMap *param_omap, cudaStream_t st);
 
 // ---- 2-SM tensor-core kernel (tc_pair_correlator.cu) ----
 // Units of 256 x 256 elements (tyx = ty2 | tx2 << 10, 128-element tile pairs),
@@ -158,7 +168,8 @@ cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStrea
 // launch, grid counts clusters and cta_offsets is indexed by cluster.
 void tc_append_pair_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t_end,
                           int tsplit, long long out_off);
-cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st);
+cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map,
+                           const CUtensorMap *param_omap, cudaStream_t st);
 
 // Tensor-core tile variants (CHX_OPT_TILE).
 constexpr int kTile1Sm = 1;  // 128 x 256 elements per CTA

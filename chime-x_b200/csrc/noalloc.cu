@@ -37,7 +37,7 @@ constexpr size_t kOffChans = 256;
 constexpr size_t kOffUnits = kOffChans + sizeof(ChanDesc) * kNoAllocMaxChannels;
 constexpr size_t kOffOffsets = kOffUnits + sizeof(Unit) * kNoAllocMaxUnits;
 constexpr int kNoAllocMaxGrid = 1024;
-constexpr size_t kScratchBytes = kOffOffsets + sizeof(int) * (kNoAllocMaxGrid + 1);  // ~144 KiB
+constexpr size_t kScratchBytes = kOffOffsets + sizeof(int) * (kNoAllocMaxGrid + 1);  // ~162 KiB
 
 // The scratch: error word, channel table, unit table.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -84,6 +84,8 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
                     upper_triangle_convention);
     if ((reinterpret_cast<uintptr_t>(d_packed) & 15) != 0)
         return fail(CHX_E_INVALID, "packed input must be 16-byte aligned for TMA");
+    if ((reinterpret_cast<uintptr_t>(d_blocks) & 15) != 0)
+        return fail(CHX_E_INVALID, "block buffer must be 16-byte aligned for TMA");
     if (F > kNoAllocMaxChannels)
         return fail(CHX_E_UNSUPPORTED, "no-allocation entry point takes at most %d channels (F=%d)",
                     kNoAllocMaxChannels, F);
@@ -115,6 +117,7 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
         chans[f].E = E;
         chans[f].nb1 = E / 32;
         chans[f].fcoord = f;
+        chans[f].orow = (int)((int64_t)f * nb * 32);
     }
     Unit *units = g_host_sorted;
     int n = 0;
@@ -160,9 +163,11 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
     if (chunks > 1 && !accumulate)
         CHX_CUDA(cudaMemsetAsync(d_blocks, 0, (size_t)F * nb * 2048 * 4, st));
 
-    CUtensorMap tmap;
-    const int r = tc_encode_map(&tmap, d_packed, E, F, T, E, (int64_t)F * E);
+    CUtensorMap tmap, omap;
+    int r = tc_encode_map(&tmap, d_packed, E, F, T, E, (int64_t)F * E);
     if (r != 0) return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", r);
+    r = tc_encode_out_map(&omap, d_blocks, (int64_t)F * nb * 32);
+    if (r != 0) return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled (blocks) failed (%d)", r);
     TcLaunch L;
     L.chans = reinterpret_cast<const ChanDesc *>(dscr + kOffChans);
     L.units = reinterpret_cast<const Unit *>(dscr + kOffUnits);
@@ -175,6 +180,6 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
     L.accumulate = accumulate ? 1 : 0;
     L.err = reinterpret_cast<int *>(dscr + kOffErr);
     L.grid = grid;
-    CHX_CUDA(tc_launch(L, &tmap, st));
+    CHX_CUDA(tc_launch(L, &tmap, &omap, st));
     return CHX_OK;
 }

@@ -12,13 +12,19 @@
 // channels whose integration completes are correlated by one persistent
 // tensor-core launch over all their work units: the integration's samples
 // accumulate in TMEM and each dump buffer is written once, so the resident
-// state never travels through HBM per frame.  A host callback after the launch
-// records, per integration, the latency from its last frame's arrival to the
-// completed dump.
+// state never travels through HBM per frame.  An event recorded after each
+// launch is watched by the stream's completion thread, which records, per
+// integration, the latency from its last frame's arrival to the moment the
+// completed dump is visible to the host (the compute stream itself never waits
+// on the host).
 #include <time.h>
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "chimex_internal.h"
@@ -42,7 +48,7 @@ struct StreamChan {
     int filled = 0;              // samples in that half
     int64_t seq = 0;             // integrations completed (dispatched)
     int64_t last_arrival = 0;
-    // published by the completion callback
+    // published by the completion thread
     int64_t done_seq = -1;
     int done_half = 0;
 };
@@ -56,13 +62,14 @@ struct Slot {
 };
 constexpr int kSlots = 8;
 
+// The integrations one launch completes, and the event recorded after it.
 struct Pending {
     struct Item {
         int chan, half;
         int64_t seq, arrival;
     };
     std::vector<Item> items;
-    struct chx_stream *owner;
+    cudaEvent_t ev = nullptr;
 };
 
 }  // namespace
@@ -81,28 +88,65 @@ struct chx_stream {
     int next_slot = 0;
     int *d_err = nullptr;
     int64_t frames = 0, dumps = 0;
-    std::mutex mu;             // guards latencies and done_* fields
+    std::mutex mu;  // guards latencies, dumps, done_* fields, queue and spare
+    std::condition_variable cv;       // new launch queued, or stop
+    std::condition_variable cv_done;  // a launch was published
     std::vector<double> latencies_ms;
-    std::vector<Pending *> inflight;
+    std::deque<Pending *> queue;   // launches in submission order
+    std::vector<Pending *> spare;  // completed records for reuse
+    std::thread poller;
+    bool stop = false;
 };
 
 namespace {
 
-void CUDART_CB on_launch_done(void *arg) {
-    Pending *p = static_cast<Pending *>(arg);
-    const int64_t t = now_ns();
-    chx_stream *s = p->owner;
-    std::lock_guard<std::mutex> lock(s->mu);
-    for (const auto &it : p->items) {
-        s->latencies_ms.push_back((double)(t - it.arrival) * 1e-6);
-        StreamChan &c = s->chans[it.chan];
-        if (it.seq > c.done_seq) {
-            c.done_seq = it.seq;
-            c.done_half = it.half;
+// Completion thread: waits (spinning on cudaEventQuery) for each launch in
+// order and publishes its dumps with their latency.
+void poll_loop(chx_stream *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (true) {
+        s->cv.wait(lk, [s] { return s->stop || !s->queue.empty(); });
+        if (s->queue.empty()) break;  // stopping with nothing left
+        Pending *p = s->queue.front();
+        lk.unlock();
+        cudaError_t q;
+        while ((q = cudaEventQuery(p->ev)) == cudaErrorNotReady) std::this_thread::yield();
+        const int64_t t = now_ns();
+        lk.lock();
+        s->queue.pop_front();
+        if (q == cudaSuccess) {
+            for (const auto &it : p->items) {
+                s->latencies_ms.push_back((double)(t - it.arrival) * 1e-6);
+                StreamChan &c = s->chans[it.chan];
+                if (it.seq > c.done_seq) {
+                    c.done_seq = it.seq;
+                    c.done_half = it.half;
+                }
+                s->dumps++;
+            }
         }
-        s->dumps++;
+        p->items.clear();
+        s->spare.push_back(p);
+        s->cv_done.notify_all();
     }
-    p->items.clear();
+}
+
+// Waits until the completion thread has published every launch queued so far.
+bool wait_published(chx_stream *s, int64_t timeout_ms) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    return s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                               [s] { return s->queue.empty(); });
+}
+
+void stop_poller(chx_stream *s) {
+    if (!s->poller.joinable()) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    s->poller.join();
 }
 
 void free_stream(chx_stream *s) {
@@ -118,8 +162,16 @@ void free_stream(chx_stream *s) {
         sl = Slot();
     }
     if (s->d_err) cudaFree(s->d_err);
-    for (Pending *p : s->inflight) delete p;
-    s->inflight.clear();
+    for (Pending *p : s->queue) {
+        if (p->ev) cudaEventDestroy(p->ev);
+        delete p;
+    }
+    for (Pending *p : s->spare) {
+        if (p->ev) cudaEventDestroy(p->ev);
+        delete p;
+    }
+    s->queue.clear();
+    s->spare.clear();
 }
 
 }  // namespace
@@ -161,6 +213,13 @@ int chx_stream_create(chx_stream **out, int max_channels, int frame_len, int ut,
         return cuda_fail(e, "stream set-up");
     }
     s->resident = (int64_t)max_channels * sizeof(ChanDesc);
+    try {
+        s->poller = std::thread(poll_loop, s);
+    } catch (...) {
+        free_stream(s);
+        delete s;
+        return fail(CHX_E_NOMEM, "cannot start the completion thread");
+    }
     *out = s;
     return CHX_OK;
 }
@@ -218,6 +277,13 @@ int chx_stream_admit(chx_stream *s, int E, int TA, int *channel_id) {
         cudaFree(c.dumps);
         return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", r);
     }
+    const int r2 = tc_encode_out_map(&d.omap, c.dumps, 2 * NB * 32);
+    if (r2 != 0) {
+        cudaFree(c.ring);
+        cudaFree(c.dumps);
+        return fail(CHX_E_CUDA, "cuTensorMapEncodeTiled (dumps) failed (%d)", r2);
+    }
+    d.orow = 0;
     d.out = (uint64_t)c.dumps;
     d.E = E;
     d.nb1 = E / 32;
@@ -270,14 +336,34 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     if (!s || (n > 0 && !ids)) return fail(CHX_E_INVALID, "NULL argument");
     DeviceGuard g(s->device);
     cudaStream_t st = (cudaStream_t)stream;
-    Pending *pend = new (std::nothrow) Pending();
-    if (!pend) return fail(CHX_E_NOMEM, "host allocation failed");
-    pend->owner = s;
+    Pending *pend = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (!s->spare.empty()) {
+            pend = s->spare.back();
+            s->spare.pop_back();
+        }
+    }
+    if (!pend) {
+        pend = new (std::nothrow) Pending();
+        if (!pend) return fail(CHX_E_NOMEM, "host allocation failed");
+        const cudaError_t e = cudaEventCreateWithFlags(&pend->ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            delete pend;
+            return cuda_fail(e, "completion event");
+        }
+    }
+    // Returns an unused record to the spare list.
+    auto drop = [s](Pending *p) {
+        p->items.clear();
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->spare.push_back(p);
+    };
     std::vector<Unit> units;
     for (int i = 0; i < n; i++) {
         const int id = ids[i];
         if (id < 0 || id >= (int)s->chans.size()) {
-            delete pend;
+            drop(pend);
             return fail(CHX_E_INVALID, "channel id %d", id);
         }
         StreamChan &c = s->chans[id];
@@ -287,7 +373,7 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
             const cudaError_t e = cudaMemcpyAsync(slot, src, (size_t)s->frame_len * c.E,
                                                   cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) {
-                delete pend;
+                drop(pend);
                 return cuda_fail(e, "frame copy");
             }
         }
@@ -303,7 +389,7 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
         }
     }
     if (units.empty()) {
-        delete pend;
+        drop(pend);
         return CHX_OK;
     }
     const int slots = std::max(1, s->sm_count / 2);
@@ -313,16 +399,22 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     const size_t ub = units.size() * sizeof(Unit);
     const size_t tb = ub + offsets.size() * sizeof(int);
     if (tb > s->slot_cap) {
-        delete pend;
+        drop(pend);
         return fail(CHX_E_INVALID, "unit table overflow");
     }
     // Reuse the oldest slot once the launch that read it has finished.
     Slot &sl = s->slots[s->next_slot];
     s->next_slot = (s->next_slot + 1) % kSlots;
-    CHX_CUDA(cudaEventSynchronize(sl.done));
-    memcpy(sl.host, units.data(), ub);
-    memcpy((char *)sl.host + ub, offsets.data(), offsets.size() * sizeof(int));
-    CHX_CUDA(cudaMemcpyAsync(sl.dev, sl.host, tb, cudaMemcpyHostToDevice, st));
+    cudaError_t e = cudaEventSynchronize(sl.done);
+    if (e == cudaSuccess) {
+        memcpy(sl.host, units.data(), ub);
+        memcpy((char *)sl.host + ub, offsets.data(), offsets.size() * sizeof(int));
+        e = cudaMemcpyAsync(sl.dev, sl.host, tb, cudaMemcpyHostToDevice, st);
+    }
+    if (e != cudaSuccess) {
+        drop(pend);
+        return cuda_fail(e, "unit table upload");
+    }
     TcLaunch L;
     L.chans = s->d_chans;
     L.units = (const Unit *)sl.dev;
@@ -335,21 +427,18 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     L.accumulate = 0;
     L.err = s->d_err;
     L.grid = grid;
-    CHX_CUDA(tc_pair_launch(L, nullptr, st));
-    CHX_CUDA(cudaEventRecord(sl.done, st));
-    CHX_CUDA(cudaLaunchHostFunc(st, on_launch_done, pend));
-    s->inflight.push_back(pend);
-    if (s->inflight.size() > 64) {  // reclaim records whose callback has run
-        std::lock_guard<std::mutex> lock(s->mu);
-        std::vector<Pending *> keep;
-        for (Pending *p : s->inflight) {
-            if (p->items.empty() && p != pend)
-                delete p;
-            else
-                keep.push_back(p);
-        }
-        s->inflight.swap(keep);
+    e = tc_pair_launch(L, nullptr, nullptr, st);
+    if (e == cudaSuccess) e = cudaEventRecord(sl.done, st);
+    if (e == cudaSuccess) e = cudaEventRecord(pend->ev, st);
+    if (e != cudaSuccess) {
+        drop(pend);
+        return cuda_fail(e, "stream launch");
     }
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->queue.push_back(pend);
+    }
+    s->cv.notify_one();
     return CHX_OK;
 }
 
@@ -400,11 +489,21 @@ int chx_stream_reset_stats(chx_stream *s) {
     return CHX_OK;
 }
 
+int chx_stream_sync(chx_stream *s) {
+    clear_error();
+    if (!s) return fail(CHX_E_INVALID, "NULL stream");
+    if (!wait_published(s, 60000))
+        return fail(CHX_E_TIMEOUT, "launches still unpublished after 60 s");
+    return CHX_OK;
+}
+
 int chx_stream_check(chx_stream *s) {
     clear_error();
     if (!s) return fail(CHX_E_INVALID, "NULL stream");
     DeviceGuard g(s->device);
     CHX_CUDA(cudaDeviceSynchronize());
+    if (!wait_published(s, 60000))
+        return fail(CHX_E_TIMEOUT, "launches still unpublished after 60 s");
     int h = 0;
     CHX_CUDA(cudaMemcpy(&h, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) {
@@ -419,6 +518,7 @@ int chx_stream_destroy(chx_stream *s) {
     if (!s) return CHX_OK;
     DeviceGuard g(s->device);
     cudaDeviceSynchronize();
+    stop_poller(s);
     free_stream(s);
     delete s;
     return CHX_OK;

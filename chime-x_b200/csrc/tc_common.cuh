@@ -83,6 +83,35 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// TMA: 2-D tile {32 words, 32 rows} of the block output from shared memory
+// (128-byte swizzled), stored or added (s32) into global memory.  One thread
+// issues it; completion is tracked with the issuing thread's bulk groups.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, uint32_t src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::
+                     "l"(reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_add_2d(const CUtensorMap *map, uint32_t src, int x, int y) {
+    asm volatile(
+        "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group"
+        " [%0, {%1, %2}], [%3];" ::"l"(reinterpret_cast<uint64_t>(map)),
+        "r"(x), "r"(y), "r"(src)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Waits until at most N of this thread's bulk groups still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// Waits until every bulk group of this thread has completed its writes.
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // Shared-memory matrix descriptor: start, leading and stride byte offsets in
 // 16-byte units, descriptor version 1, 128-byte swizzle (layout type 2).
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -139,6 +168,19 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c),
                  "r"(d)
                  : "memory");
+}
+
+// Writes one row (lane) of a 32 x 32-word staging tile: 16 (Re, Im) pairs
+// as eight 16-byte chunks, chunk c at position c ^ (row & 7) (the 128-byte
+// swizzle of the output tensor map), so the warp's stores hit every bank.
+__device__ __forceinline__ void stage_row(uint32_t tile, int row, const uint32_t (&re)[16],
+                                          const uint32_t (&im)[16]) {
+    const uint32_t base = tile + (uint32_t)row * 128u;
+    const uint32_t x = (uint32_t)(row & 7);
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+        sts128(base + (((uint32_t)c ^ x) << 4), re[2 * c], im[2 * c], re[2 * c + 1],
+               im[2 * c + 1]);
 }
 
 // ------------------------------------------------------------- SWAR unpack

@@ -72,6 +72,8 @@ constexpr int kOffPkY = kOffOpX + kOpStages * kXOpBytes;
 constexpr int kOffPkX = kOffPkY + kPkStages * kPkYBytes;
 constexpr int kOffBars = kOffPkX + kPkStages * kPkXBytes;
 constexpr int kSmemBytes = kOffBars + 256 + 1024;
+// Epilogue staging (8 KiB per unpack warp) reuses the operand slots.
+static_assert(kUnpackWarps * 8192 <= kOffPkY - kOffOpY, "epilogue staging");
 
 struct KParams {
     const ChanDesc *chans;
@@ -87,7 +89,8 @@ struct KParams {
 
 template <int MAP>
 __global__ void __launch_bounds__(kThreads, 1)
-tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
+tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
+                    const __grid_constant__ CUtensorMap pomap, const KParams P) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -105,6 +108,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
     const uint32_t drain = acc_full + 16;
     volatile uint32_t *tmem_slot = reinterpret_cast<volatile uint32_t *>(
         smem + kOffBars + 8 * (2 * kPkStages + kOpStages + 5));
+    const uint32_t epi_done = bars + 8 * (2 * kPkStages + kOpStages + 6);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -120,6 +124,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         mbar_init(acc_full, 1);
         mbar_init(acc_empty, kUnpackThreads);
         mbar_init(drain, 1);
+        mbar_init(epi_done, kUnpackWarps);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -260,8 +265,11 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         const uint32_t ry = (uint32_t)(sy & 7), by8 = (uint32_t)(sy >> 3);
         const uint32_t ldoff = (uint32_t)(sy * 128 + gy * 16);
         const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);  // R (y) or X (x); I / Y at +1K
-        uint32_t g = 0, gp_base = 0, acc_phase = 0;
+        uint32_t g = 0, gp_base = 0, acc_phase = 0, epi_phase = 0;
         bool ok = true;
+        // Epilogue staging: 8 KiB per warp inside the operand slots, which
+        // are idle from the accumulator commit until the next unit's unpack.
+        const uint32_t stage = op_y + (uint32_t)warp * 8192u;
         for (int u = first; u < last && ok; u++) {
             const Unit U = P.units[u];
             const ChanDesc *cd = P.chans + U.chan;
@@ -352,15 +360,16 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
             const int q = warp & 3, h = warp >> 2;  // lane quarter, column group
             const int nb1 = cd->nb1;
             const int by = ty * 4 + q;
-            int32_t *out = reinterpret_cast<int32_t *>(P.out_base + cd->out) + U.out_off;
             const int mode = U.split ? 2 : (P.accumulate ? 1 : 0);
+            const CUtensorMap *omap = P.use_param_map ? &pomap : &cd->omap;
+            const int row0 = cd->orow + (int)(U.out_off >> 6);
+            uint32_t nchunk = 0;
 #pragma unroll 1
             for (int jj = 0; jj < nx; jj++) {
                 const int j = h * nx + jj;  // 32-column x block
                 const int bx = x0 * 4 + j;
-                const bool store = !(by >= nb1 || bx >= nb1 || bx < by);
+                if (by >= nb1 || bx >= nb1 || bx < by) continue;  // warp-uniform
                 const int64_t b = (int64_t)by * nb1 - (int64_t)by * (by - 1) / 2 + (bx - by);
-                int32_t *dst = out + (b * 32 + lane) * 64;
                 const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + 32 * j;
 #pragma unroll 1
                 for (int half = 0; half < 2; half++) {
@@ -368,45 +377,59 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                     tmem_ld16(taddr + 16 * half, re);
                     tmem_ld16(taddr + 256 + 16 * half, im);
                     tmem_wait_ld();
-                    if (!store) continue;
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
                         re[k] = (uint32_t)((int32_t)re[k] >> 4);
                         im[k] = (uint32_t)((int32_t)im[k] >> 4);
                         if (!P.ut) im[k] = 0u - im[k];
                     }
-                    int32_t *d = dst + 32 * half;
-                    if (mode == 0) {
-#pragma unroll
-                        for (int k = 0; k < 16; k += 2)
-                            *reinterpret_cast<int4 *>(d + 2 * k) =
-                                make_int4((int)re[k], (int)im[k], (int)re[k + 1], (int)im[k + 1]);
-                    } else if (mode == 1) {
-#pragma unroll
-                        for (int k = 0; k < 16; k += 2) {
-                            int4 o = *reinterpret_cast<int4 *>(d + 2 * k);
-                            o.x = (int)((uint32_t)o.x + re[k]);
-                            o.y = (int)((uint32_t)o.y + im[k]);
-                            o.z = (int)((uint32_t)o.z + re[k + 1]);
-                            o.w = (int)((uint32_t)o.w + im[k + 1]);
-                            *reinterpret_cast<int4 *>(d + 2 * k) = o;
-                        }
-                    } else {
+                    if (mode == 2) {  // split units: other units add to these cells
+                        int32_t *d = reinterpret_cast<int32_t *>(P.out_base + cd->out) +
+                                     U.out_off + (b * 32 + lane) * 64 + 32 * half;
 #pragma unroll
                         for (int k = 0; k < 16; k++) {
                             atomicAdd(d + 2 * k, (int)re[k]);
                             atomicAdd(d + 2 * k + 1, (int)im[k]);
                         }
+                        continue;
                     }
+                    // Stage the 32 x 32-word tile (rows = lanes) and hand it to
+                    // TMA; two staging tiles alternate.
+                    const uint32_t tile = stage + (nchunk & 1u) * 4096u;
+                    if (lane == 0) bulk_wait_read<1>();
+                    __syncwarp();
+                    stage_row(tile, lane, re, im);
+                    fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0) {
+                        const int y = row0 + (int)b * 32;
+                        if (mode == 0)
+                            tma_store_2d(omap, tile, 32 * half, y);
+                        else
+                            tma_add_2d(omap, tile, 32 * half, y);
+                        bulk_commit();
+                    }
+                    nchunk++;
                 }
             }
+            if (lane == 0) bulk_wait_read<0>();  // staging read by TMA
             tc_fence_before();
+            __syncwarp();
             mbar_arrive(acc_empty);
+            if (lane == 0) mbar_arrive(epi_done);
+            // The next unit's unpack overwrites the staging tiles: wait until
+            // every warp's tiles have been read.
+            if (!mbar_wait(epi_done, epi_phase, abort_flag)) {
+                ok = false;
+                break;
+            }
+            epi_phase ^= 1;
         }
         if (!ok) {
             atomicOr(P.err, 0x40);
             *abort_flag = 1;
         }
+        if (lane == 0) bulk_wait_all();  // output tiles written
     }
 
     tc_fence_before();
@@ -420,7 +443,8 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
 }
 
 template <int MAP>
-cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, cudaStream_t st) {
+cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, const CUtensorMap *pomap,
+                       cudaStream_t st) {
     // The shared-memory opt-in is a per-device function attribute.
     static bool attr_done[64] = {};
     int dev = 0;
@@ -445,7 +469,8 @@ cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, cudaStream_t 
     P.err = L.err;
     CUtensorMap dummy;
     memset(&dummy, 0, sizeof(dummy));
-    tc_correlate_kernel<MAP><<<L.grid, kThreads, kSmemBytes, st>>>(pmap ? *pmap : dummy, P);
+    tc_correlate_kernel<MAP><<<L.grid, kThreads, kSmemBytes, st>>>(
+        pmap ? *pmap : dummy, pomap ? *pomap : dummy, P);
     return cudaGetLastError();
 }
 
@@ -536,13 +561,37 @@ int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t
     return r == CUDA_SUCCESS ? 0 : (int)r;
 }
 
-cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st) {
+int tc_encode_out_map(CUtensorMap *m, void *base, int64_t rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            return -1;
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    if (!tc_out_rows_ok(rows) || (reinterpret_cast<uintptr_t>(base) & 15)) return -2;
+    cuuint64_t dims[2] = {64, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {256};
+    cuuint32_t box[2] = {32, 32};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_INT32, 2, base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
+cudaError_t tc_launch(const TcLaunch &L, const CUtensorMap *param_map,
+                      const CUtensorMap *param_omap, cudaStream_t st) {
     if (L.nunits <= 0) return cudaSuccess;
     if (L.grid <= 0) return cudaErrorInvalidValue;
+    if (L.use_param_map && (!param_map || !param_omap)) return cudaErrorInvalidValue;
     switch (L.map) {
-    case MAP_EXACT: return launch_map<MAP_EXACT>(L, param_map, st);
-    case MAP_CONF: return launch_map<MAP_CONF>(L, param_map, st);
-    default: return launch_map<MAP_PACKED>(L, param_map, st);
+    case MAP_EXACT: return launch_map<MAP_EXACT>(L, param_map, param_omap, st);
+    case MAP_CONF: return launch_map<MAP_CONF>(L, param_map, param_omap, st);
+    default: return launch_map<MAP_PACKED>(L, param_map, param_omap, st);
     }
 }
 

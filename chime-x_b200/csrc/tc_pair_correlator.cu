@@ -15,6 +15,12 @@
 // [R0 I0 R1 I1 R2 I2 R3 I3 | I0 N0 I1 N1 I2 N2 I3 N3] (16 KiB) and x
 // [X0 Y0 X1 Y1 X2 Y2 X3 Y3] (8 KiB).
 //
+// Warps: 0-15 unpack (0-7 y, 8-15 x), 16 TMA producer, 17 MMA issuer (CTA 0),
+// 18-25 epilogue.  The epilogue warps drain the accumulators of one unit while
+// the unpack warps convert the next; each 32 x 32-word output tile goes from
+// TMEM through a swizzled staging tile in shared memory to a TMA store (or
+// reduce-add) into the block buffer.
+//
 // Synchronisation across the pair:
 //   full_pair[p] in CTA 0; every unpack warp of both CTAs arrives once per
 //                stage pair (one lane, after its lanes' proxy fences) -> the
@@ -41,23 +47,30 @@ using namespace tc;
 constexpr int kStageSamples = 32;
 constexpr int kOpSlots = 6;     // 3 stage pairs
 constexpr int kPairs = kOpSlots / 2;
-constexpr int kPkStages = 10;
+constexpr int kPkStages = 6;
 constexpr int kYOpBytes = 16 * 1024;
 constexpr int kXOpBytes = 8 * 1024;
 constexpr int kPkBytes = kStageSamples * 128;  // one 128-element tile, 4 KiB
 constexpr int kUnpackWarps = 16;
-constexpr int kUnpackThreads = kUnpackWarps * 32;
 constexpr int kProducerWarp = 16;
 constexpr int kMmaWarp = 17;
-constexpr int kThreads = 576;
+constexpr int kEpiWarp0 = 18;   // epilogue warps from here on, lane quarter = warp % 4
+constexpr int kEpiWarps = 8;    // 4 or 8: each warp drains 8 / (kEpiWarps / 4) column blocks
+constexpr int kEpiTiles = 1;    // 4 KiB output staging tiles per epilogue warp
+constexpr int kEpiStageBytes = kEpiTiles * 4096;
+constexpr int kEpiBlocks = 8 / (kEpiWarps / 4);
+constexpr int kThreads = (kEpiWarp0 + kEpiWarps) * 32;
+static_assert(kEpiWarps == 4 || kEpiWarps == 8, "epilogue warps");
 constexpr int kTmemCols = 512;
 
 constexpr int kOffOpY = 0;
 constexpr int kOffOpX = kOffOpY + kOpSlots * kYOpBytes;
 constexpr int kOffPkY = kOffOpX + kOpSlots * kXOpBytes;
 constexpr int kOffPkX = kOffPkY + kPkStages * kPkBytes;
-constexpr int kOffBars = kOffPkX + kPkStages * kPkBytes;
+constexpr int kOffStage = kOffPkX + kPkStages * kPkBytes;
+constexpr int kOffBars = kOffStage + kEpiWarps * kEpiStageBytes;
 constexpr int kSmemBytes = kOffBars + 256 + 1024;
+static_assert(kSmemBytes <= 232448, "shared memory per CTA");
 
 // Barrier offsets inside the barrier block (8 bytes each).
 constexpr int kBarFullPk = 0;
@@ -146,7 +159,8 @@ struct KParams {
 
 template <int MAP>
 __global__ void __launch_bounds__(kThreads, 1)
-tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
+tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap pomap,
+               const KParams P) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -171,7 +185,7 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         for (int s = 0; s < kPairs; s++) mbar_init(bar(kBarFullPair + s), 2 * kUnpackWarps);
         for (int s = 0; s < kPairs; s++) mbar_init(bar(kBarEmptyPair + s), 1);
         mbar_init(bar(kBarAccFull), 1);
-        mbar_init(bar(kBarAccEmpty), 2 * kUnpackWarps);
+        mbar_init(bar(kBarAccEmpty), 2 * kEpiWarps);
         mbar_init(bar(kBarDrain), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -299,8 +313,8 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
             (void)ncommit;
         }
         __syncwarp();
-    } else {
-        // ------------------------------------------------- unpack + epilogue (both CTAs)
+    } else if (warp < kUnpackWarps) {
+        // ------------------------------------------------- unpack (both CTAs)
         const int tid = threadIdx.x;  // 0..511
         const bool is_y = tid < 256;
         const int c = tid & 255;
@@ -309,15 +323,11 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         const uint32_t ldoff = (uint32_t)(sy * 128 + gy * 16);
         const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);
         const uint32_t full_pair_leader = mapa(bar(kBarFullPair), 0);
-        const uint32_t acc_empty_leader = mapa(bar(kBarAccEmpty), 0);
-        uint32_t g = 0, gp = 0, acc_phase = 0;
+        uint32_t g = 0, gp = 0;
         uint32_t npairs_done[kPairs] = {};
         bool ok = true;
         for (int u = first; u < last && ok; u++) {
             const Unit U = P.units[u];
-            const ChanDesc *cd = P.chans + U.chan;
-            const int ty = 2 * (U.tyx & 1023) + (int)rank;
-            const int tx2 = (U.tyx >> 10) & 1023;
             const int nst = (U.t1 - U.t0 + kStageSamples - 1) / kStageSamples;
             // Stages are unpacked two at a time (one stage pair): both loads
             // and conversions first, then one wait for the operand slots, the
@@ -389,69 +399,6 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
                 if (lane == 0) mbar_arrive_cluster(full_pair_leader + 8 * pslot);
                 npairs_done[pslot]++;
             }
-            if (!ok) break;
-
-            // -------------------------------------------------- epilogue
-            if (!mbar_wait(bar(kBarAccFull), acc_phase, abort_flag)) {
-                ok = false;
-                break;
-            }
-            acc_phase ^= 1;
-            tc_fence_after();
-            const int q = warp & 3, h = warp >> 2;
-            const int nb1 = cd->nb1;
-            const int by = ty * 4 + q;
-            int32_t *out = reinterpret_cast<int32_t *>(P.out_base + cd->out) + U.out_off;
-            const int mode = U.split ? 2 : (P.accumulate ? 1 : 0);
-#pragma unroll 1
-            for (int jj = 0; jj < 2; jj++) {
-                const int j = h * 2 + jj;  // 32-column block within the 256 x columns
-                const int bx = tx2 * 8 + j;
-                const bool store = !(by >= nb1 || bx >= nb1 || bx < by);
-                const int64_t b = (int64_t)by * nb1 - (int64_t)by * (by - 1) / 2 + (bx - by);
-                int32_t *dst = out + (b * 32 + lane) * 64;
-                const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + 32 * j;
-#pragma unroll 1
-                for (int half = 0; half < 2; half++) {
-                    uint32_t re[16], im[16];
-                    tmem_ld16(taddr + 16 * half, re);
-                    tmem_ld16(taddr + 256 + 16 * half, im);
-                    tmem_wait_ld();
-                    if (!store) continue;
-#pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        re[k] = (uint32_t)((int32_t)re[k] >> 4);
-                        im[k] = (uint32_t)((int32_t)im[k] >> 4);
-                        if (!P.ut) im[k] = 0u - im[k];
-                    }
-                    int32_t *d = dst + 32 * half;
-                    if (mode == 0) {
-#pragma unroll
-                        for (int k = 0; k < 16; k += 2)
-                            *reinterpret_cast<int4 *>(d + 2 * k) =
-                                make_int4((int)re[k], (int)im[k], (int)re[k + 1], (int)im[k + 1]);
-                    } else if (mode == 1) {
-#pragma unroll
-                        for (int k = 0; k < 16; k += 2) {
-                            int4 o = *reinterpret_cast<int4 *>(d + 2 * k);
-                            o.x = (int)((uint32_t)o.x + re[k]);
-                            o.y = (int)((uint32_t)o.y + im[k]);
-                            o.z = (int)((uint32_t)o.z + re[k + 1]);
-                            o.w = (int)((uint32_t)o.w + im[k + 1]);
-                            *reinterpret_cast<int4 *>(d + 2 * k) = o;
-                        }
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 16; k++) {
-                            atomicAdd(d + 2 * k, (int)re[k]);
-                            atomicAdd(d + 2 * k + 1, (int)im[k]);
-                        }
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_cluster(acc_empty_leader);
         }
         if (!ok) {
             atomicOr(P.err, 0x400);
@@ -462,6 +409,91 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
         if (tid == 0)
             for (int k = 0; k < kPairs; k++)
                 if (npairs_done[k]) mbar_wait_drain(bar(kBarEmptyPair + k), (npairs_done[k] - 1) & 1);
+    } else {
+        // ------------------------------------------------- epilogue (both CTAs)
+        // Epilogue warp w drains TMEM lanes 32 * (w % 4) .. +31 (its quarter of
+        // the CTA's 128 y rows) over kEpiBlocks 32-column blocks of Re and Im,
+        // hands the cells to TMA through its staging tiles, and releases the
+        // accumulator as soon as its last TMEM load completes, while the unpack
+        // warps are already converting the next unit.
+        const int q = warp & 3;
+        const int j0 = ((warp - kEpiWarp0) >> 2) * kEpiBlocks;
+        const uint32_t acc_empty_leader = mapa(bar(kBarAccEmpty), 0);
+        const uint32_t stage = sbase + kOffStage + (uint32_t)(warp - kEpiWarp0) * kEpiStageBytes;
+        uint32_t acc_phase = 0, nchunk = 0;
+        bool ok = true;
+        for (int u = first; u < last && ok; u++) {
+            const Unit U = P.units[u];
+            const ChanDesc *cd = P.chans + U.chan;
+            const int ty = 2 * (U.tyx & 1023) + (int)rank;
+            const int tx2 = (U.tyx >> 10) & 1023;
+            const int nb1 = cd->nb1;
+            const int by = ty * 4 + q;
+            const int mode = U.split ? 2 : (P.accumulate ? 1 : 0);
+            const CUtensorMap *omap = P.use_param_map ? &pomap : &cd->omap;
+            const int row0 = cd->orow + (int)(U.out_off >> 6);
+            if (!mbar_wait(bar(kBarAccFull), acc_phase, abort_flag)) {
+                ok = false;
+                break;
+            }
+            acc_phase ^= 1;
+            tc_fence_after();
+#pragma unroll 1
+            for (int j = j0; j < j0 + kEpiBlocks; j++) {  // 32-column block of the 256 x columns
+                const int bx = tx2 * 8 + j;
+                if (by >= nb1 || bx >= nb1 || bx < by) continue;  // warp-uniform
+                const int64_t b = (int64_t)by * nb1 - (int64_t)by * (by - 1) / 2 + (bx - by);
+                const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + 32 * j;
+#pragma unroll 1
+                for (int half = 0; half < 2; half++) {
+                    uint32_t re[16], im[16];
+                    tmem_ld16(taddr + 16 * half, re);
+                    tmem_ld16(taddr + 256 + 16 * half, im);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        re[k] = (uint32_t)((int32_t)re[k] >> 4);
+                        im[k] = (uint32_t)((int32_t)im[k] >> 4);
+                        if (!P.ut) im[k] = 0u - im[k];
+                    }
+                    if (mode == 2) {  // split units: other units add to these cells
+                        int32_t *d = reinterpret_cast<int32_t *>(P.out_base + cd->out) +
+                                     U.out_off + (b * 32 + lane) * 64 + 32 * half;
+#pragma unroll
+                        for (int k = 0; k < 16; k++) {
+                            atomicAdd(d + 2 * k, (int)re[k]);
+                            atomicAdd(d + 2 * k + 1, (int)im[k]);
+                        }
+                        continue;
+                    }
+                    // Stage the 32 x 32-word tile (rows = lanes) and hand it to
+                    // TMA; the staging tiles are used in turn.
+                    const uint32_t tile = stage + (nchunk % (uint32_t)kEpiTiles) * 4096u;
+                    if (lane == 0) bulk_wait_read<kEpiTiles - 1>();
+                    __syncwarp();
+                    stage_row(tile, lane, re, im);
+                    fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0) {
+                        const int y = row0 + (int)b * 32;
+                        if (mode == 0)
+                            tma_store_2d(omap, tile, 32 * half, y);
+                        else
+                            tma_add_2d(omap, tile, 32 * half, y);
+                        bulk_commit();
+                    }
+                    nchunk++;
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(acc_empty_leader);
+        }
+        if (!ok) {
+            atomicOr(P.err, 0x800);
+            *abort_flag = 1;
+        }
+        if (lane == 0) bulk_wait_all();  // output tiles written
     }
 
     tc_fence_before();
@@ -476,7 +508,8 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const KParams P) {
 }
 
 template <int MAP>
-cudaError_t launch_pair_map(const TcLaunch &L, const CUtensorMap *pmap, cudaStream_t st) {
+cudaError_t launch_pair_map(const TcLaunch &L, const CUtensorMap *pmap, const CUtensorMap *pomap,
+                            cudaStream_t st) {
     static bool attr_done[64] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -511,7 +544,8 @@ cudaError_t launch_pair_map(const TcLaunch &L, const CUtensorMap *pmap, cudaStre
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, tc_pair_kernel<MAP>, pmap ? *pmap : dummy, P);
+    e = cudaLaunchKernelEx(&cfg, tc_pair_kernel<MAP>, pmap ? *pmap : dummy, pomap ? *pomap : dummy,
+                           P);
     if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
@@ -543,13 +577,15 @@ void tc_append_pair_units(std::vector<Unit> &out, int chan, int E, int t_begin, 
             }
 }
 
-cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map, cudaStream_t st) {
+cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map,
+                           const CUtensorMap *param_omap, cudaStream_t st) {
     if (L.nunits <= 0) return cudaSuccess;
     if (L.grid <= 0) return cudaErrorInvalidValue;
+    if (L.use_param_map && (!param_map || !param_omap)) return cudaErrorInvalidValue;
     switch (L.map) {
-    case MAP_EXACT: return launch_pair_map<MAP_EXACT>(L, param_map, st);
-    case MAP_CONF: return launch_pair_map<MAP_CONF>(L, param_map, st);
-    default: return launch_pair_map<MAP_PACKED>(L, param_map, st);
+    case MAP_EXACT: return launch_pair_map<MAP_EXACT>(L, param_map, param_omap, st);
+    case MAP_CONF: return launch_pair_map<MAP_CONF>(L, param_map, param_omap, st);
+    default: return launch_pair_map<MAP_PACKED>(L, param_map, param_omap, st);
     }
 }
 

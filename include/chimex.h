@@ -248,17 +248,22 @@ int chx_stream_frame_slot(chx_stream *s, int channel_id, uint8_t **d_slot);
 int chx_stream_submit(chx_stream *s, int n, const int *channel_ids,
                       const uint8_t *const *d_frames, const int64_t *arrival_ns,
                       void *stream);
-/* Channel c's last integration whose dump has completed on the device (NULL,
- * seq -1 if none) and its sequence number.  The buffer is overwritten when
- * integration seq+2 completes. */
+/* Channel c's last integration whose dump has completed on the device and
+ * been published by the stream's completion thread (NULL, seq -1 if none),
+ * and its sequence number.  The buffer is overwritten when integration seq+2
+ * completes.  Completion is observed by a host thread that polls an event
+ * recorded after each launch; chx_stream_sync waits for it. */
 int chx_stream_last_dump(chx_stream *s, int channel_id, const int32_t **d_blocks,
                          int64_t *seq);
 /* Counters and latency percentiles over the dumps completed so far. */
 int chx_stream_stats_get(chx_stream *s, chx_stream_stats *out);
 /* Forgets the latency samples (counters stay). */
 int chx_stream_reset_stats(chx_stream *s);
-/* Synchronises the device, reads and clears the device error word.  Returns
- * CHX_OK or CHX_E_TIMEOUT. */
+/* Waits until every launch submitted so far has completed on the device and
+ * its dumps are published (chx_stream_last_dump, statistics). */
+int chx_stream_sync(chx_stream *s);
+/* Synchronises the device and the published dumps, reads and clears the
+ * device error word.  Returns CHX_OK or CHX_E_TIMEOUT. */
 int chx_stream_check(chx_stream *s);
 int chx_stream_destroy(chx_stream *s);
 

@@ -44,7 +44,7 @@ def test_stream_dumps_match_oracle(chimex):
             frames.append(torch.from_numpy(h.reshape(-1)).cuda())
             host.append(h)
         s.submit(sub, frames)
-        torch.cuda.synchronize()
+        s.sync()
         for c, h in zip(sub, host):
             history[c].append(h)
             E, ta = layout[c]
@@ -79,12 +79,12 @@ def test_stream_in_place_frames_reuse_ring(chimex):
                   for _ in range(2)]
         for f in frames:
             s.submit([c], [f])
-        torch.cuda.synchronize()
+        s.sync()
         dumps.append(dump_of(s, c)[0])
     for k in range(2):
         for _ in range(2):
             s.submit([c], None)
-        torch.cuda.synchronize()
+        s.sync()
         got, seq = dump_of(s, c)
         assert seq == 4 + k
         np.testing.assert_array_equal(got, dumps[2 + k])
