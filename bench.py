@@ -397,6 +397,10 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="tensor-core tile: 0 auto, 1 one SM, 2 SM pair")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="batched: skip the autotuner (default tiles; profiling cases)")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="batched: skip the plain per-channel comparison and e2e (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

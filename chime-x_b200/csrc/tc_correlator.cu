@@ -72,7 +72,8 @@ constexpr int kOffPkY = kOffOpX + kOpStages * kXOpBytes;
 constexpr int kOffPkX = kOffPkY + kPkStages * kPkYBytes;
 constexpr int kOffBars = kOffPkX + kPkStages * kPkXBytes;
 constexpr int kSmemBytes = kOffBars + 256 + 1024;
-// Epilogue staging (8 KiB per unpack warp) reuses the operand slots.
+// Epilogue staging (two 4 KiB tiles per unpack warp) reuses the operand slots.
+constexpr int kEpiTiles = 2;
 static_assert(kUnpackWarps * 8192 <= kOffPkY - kOffOpY, "epilogue staging");
 
 struct KParams {
@@ -373,32 +374,38 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                 const uint32_t taddr = tmem_base + ((uint32_t)(32 * q) << 16) + 32 * j;
 #pragma unroll 1
                 for (int half = 0; half < 2; half++) {
-                    uint32_t re[16], im[16];
-                    tmem_ld16(taddr + 16 * half, re);
-                    tmem_ld16(taddr + 256 + 16 * half, im);
-                    tmem_wait_ld();
-#pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        re[k] = (uint32_t)((int32_t)re[k] >> 4);
-                        im[k] = (uint32_t)((int32_t)im[k] >> 4);
-                        if (!P.ut) im[k] = 0u - im[k];
+                    // Stage the 32 x 32-word tile (rows = lanes) in two
+                    // 8-column parts, then hand it to TMA.
+                    const uint32_t tile = stage + (nchunk % (uint32_t)kEpiTiles) * 4096u;
+                    if (mode != 2) {
+                        if (lane == 0) bulk_wait_read<kEpiTiles - 1>();
+                        __syncwarp();
                     }
-                    if (mode == 2) {  // split units: other units add to these cells
-                        int32_t *d = reinterpret_cast<int32_t *>(P.out_base + cd->out) +
-                                     U.out_off + (b * 32 + lane) * 64 + 32 * half;
 #pragma unroll
-                        for (int k = 0; k < 16; k++) {
-                            atomicAdd(d + 2 * k, (int)re[k]);
-                            atomicAdd(d + 2 * k + 1, (int)im[k]);
+                    for (int part = 0; part < 2; part++) {
+                        uint32_t re[8], im[8];
+                        tmem_ld8(taddr + 16 * half + 8 * part, re);
+                        tmem_ld8(taddr + 256 + 16 * half + 8 * part, im);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            re[k] = (uint32_t)((int32_t)re[k] >> 4);
+                            im[k] = (uint32_t)((int32_t)im[k] >> 4);
+                            if (!P.ut) im[k] = 0u - im[k];
                         }
-                        continue;
+                        if (mode == 2) {  // split units: other units add to these cells
+                            int32_t *d = reinterpret_cast<int32_t *>(P.out_base + cd->out) +
+                                         U.out_off + (b * 32 + lane) * 64 + 32 * half + 16 * part;
+#pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                atomicAdd(d + 2 * k, (int)re[k]);
+                                atomicAdd(d + 2 * k + 1, (int)im[k]);
+                            }
+                        } else {
+                            stage_row_half(tile, lane, part, re, im);
+                        }
                     }
-                    // Stage the 32 x 32-word tile (rows = lanes) and hand it to
-                    // TMA; two staging tiles alternate.
-                    const uint32_t tile = stage + (nchunk & 1u) * 4096u;
-                    if (lane == 0) bulk_wait_read<1>();
-                    __syncwarp();
-                    stage_row(tile, lane, re, im);
+                    if (mode == 2) continue;
                     fence_proxy_async();
                     __syncwarp();
                     if (lane == 0) {
