@@ -190,8 +190,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
         // Im MMAs, then one commit releasing both operand slots.  Runs of
         // MMAs into one accumulator and few commits keep the tensor pipe full.
         if (lane == 0) {
-            uint32_t gp = 0, acc_phase = 0;  // pair counter
-            uint32_t ncommit[2] = {0, 0};
+            uint32_t gp = 0, acc_phase = 0;  // pair counter (pair gp uses slot gp & 1)
             bool ok = true;
             const bool b_signed = (MAP == MAP_EXACT);
             const uint64_t dRe0 = sdesc(op_y, 1024, 1024), dRe1 = sdesc(op_y + 4096, 1024, 1024);
@@ -236,7 +235,6 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                         mma_i8(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);
                     }
                     mma_commit(empty_pair(ps));
-                    ncommit[ps]++;
                 }
                 if (!ok) break;
                 mma_commit(acc_full);
@@ -250,8 +248,10 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
             }
             // No arrival may be pending when the CTA retires: wait for the
             // last phase committed on each pair barrier.
-            for (int k = 0; k < 2; k++)
-                if (ncommit[k]) mbar_wait_drain(empty_pair(k), (ncommit[k] - 1) & 1);
+            for (uint32_t k = 0; k < 2; k++) {
+                const uint32_t ncommit = gp > k ? (gp - 1 - k) / 2 + 1 : 0;  // commits on slot k
+                if (ncommit) mbar_wait_drain(empty_pair(k), (ncommit - 1) & 1);
+            }
         }
         __syncwarp();
     } else {

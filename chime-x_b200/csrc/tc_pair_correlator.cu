@@ -244,7 +244,6 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
     } else if (warp == kMmaWarp) {
         // ------------------------------------------------- MMA issuer (CTA 0 only)
         if (lane == 0) {
-            uint32_t ncommit[kPairs] = {};
             if (rank == 0) {
                 uint32_t gp = 0, acc_phase = 0;
                 bool ok = true;
@@ -294,7 +293,6 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                             mma_i8_pair(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);
                         }
                         mma_commit_pair(bar(kBarEmptyPair + ps));
-                        ncommit[ps]++;
                     }
                     if (!ok) break;
                     mma_commit_pair(bar(kBarAccFull));
@@ -310,7 +308,6 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                     mbar_wait_drain(bar(kBarDrain), 0);
                 }
             }
-            (void)ncommit;
         }
         __syncwarp();
     } else if (warp < kUnpackWarps) {
@@ -324,7 +321,6 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
         const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);
         const uint32_t full_pair_leader = mapa(bar(kBarFullPair), 0);
         uint32_t g = 0, gp = 0;
-        uint32_t npairs_done[kPairs] = {};
         bool ok = true;
         for (int u = first; u < last && ok; u++) {
             const Unit U = P.units[u];
@@ -397,7 +393,6 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                 fence_proxy_async();
                 __syncwarp();
                 if (lane == 0) mbar_arrive_cluster(full_pair_leader + 8 * pslot);
-                npairs_done[pslot]++;
             }
         }
         if (!ok) {
@@ -408,7 +403,8 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
         // barriers when it retires: thread 0 waits for the last phase of each.
         if (tid == 0)
             for (int k = 0; k < kPairs; k++)
-                if (npairs_done[k]) mbar_wait_drain(bar(kBarEmptyPair + k), (npairs_done[k] - 1) & 1);
+                if (gp > (uint32_t)k)  // pairs gp' < gp with slot k: their last phase
+                    mbar_wait_drain(bar(kBarEmptyPair + k), ((gp - 1 - k) / kPairs) & 1);
     } else {
         // ------------------------------------------------- epilogue (both CTAs)
         // Epilogue warp w drains TMEM lanes 32 * (w % 4) .. +31 (its quarter of
