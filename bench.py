@@ -65,6 +65,21 @@ def int8_peak(peaks):
     return 2.0 * 1590.0, "2 x fallback bf16 1.59 PF/s"
 
 
+def profile_traffic(name):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    recorded from one ncu capture of this workload in profiles/<name>; None
+    when there is no summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
     """Samples SM clocks and throttle reasons with nvidia-smi while running."""
@@ -279,12 +294,15 @@ def run_plain(args, torch, cx, dist):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_reference_rate(E, 1536)
+        r = cpu_reference_rate(E, 3072)
         if r is not None:
             cpu = {"value": r[0] / 1e12, "unit": "TOPS", "cores": r[1], "kind": r[3],
                    "sample": r[2], "seconds": round(r[4], 2)}
 
     peak, peak_src = int8_peak(load_peaks())
+    traffic = None
+    if (E, F, T) == (2048, 8, 16384) and args.algo != "simt" and args.tile in (0, 2):
+        traffic = profile_traffic("tc_pair_correlate_E2048_F8_T16384.md")
     kernel_ms = sorted(per_launch)[len(per_launch) // 2]
     achieved = ops_step / (sum(per_launch) / len(per_launch) * 1e-3) / 1e12
     line = {
@@ -300,7 +318,7 @@ def run_plain(args, torch, cx, dist):
                        E * F * T >> 20, "larger than" if E * F * T > 126e6 else "SMALLER than"),
                    "parallelism": "channel shards, %d GPU(s), no collective" % world},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
-                     "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "kernel": "correlator", "median_launch_ms": kernel_ms,
                      "nominal_peak": NOMINAL_INT8_TOPS},
         "pct_of_int8_peak": 100.0 * value / world / peak,

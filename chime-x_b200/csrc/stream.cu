@@ -62,6 +62,33 @@ struct Slot {
 };
 constexpr int kSlots = 8;
 
+// One frame copied into a ring slot (device addresses, 16-byte aligned, bytes
+// a multiple of 16).
+struct FrameCopy {
+    const uint8_t *src;
+    uint8_t *dst;
+    int64_t bytes;
+};
+
+// All frame copies of one submit in one launch: block y = copy, blocks x
+// stride over its 16-byte words.
+__global__ void frame_copy_kernel(const FrameCopy *copies) {
+    const FrameCopy c = copies[blockIdx.y];
+    const int64_t words = c.bytes >> 4;
+    const uint4 *src = reinterpret_cast<const uint4 *>(c.src);
+    uint4 *dst = reinterpret_cast<uint4 *>(c.dst);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words;
+         i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = __ldg(src + i);
+}
+
+cudaError_t launch_frame_copies(const FrameCopy *d_copies, int n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (n > 65535) return cudaErrorInvalidValue;
+    frame_copy_kernel<<<dim3(8, n), 256, 0, st>>>(d_copies);
+    return cudaGetLastError();
+}
+
 // The integrations one launch completes, and the event recorded after it.
 struct Pending {
     struct Item {
@@ -84,7 +111,7 @@ struct chx_stream {
     ChanDesc *d_chans = nullptr;
     std::vector<ChanDesc> h_chans;
     Slot slots[kSlots];
-    size_t slot_cap = 0;  // bytes per slot: units + offsets
+    size_t slot_cap = 0;  // bytes per slot: units, offsets, frame copies
     int next_slot = 0;
     int *d_err = nullptr;
     int64_t frames = 0, dumps = 0;
@@ -295,7 +322,8 @@ int chx_stream_admit(chx_stream *s, int E, int TA, int *channel_id) {
     // once.  Growing waits for all launches that read the old tables.
     size_t total_units = c.units[0].size();
     for (const auto &x : s->chans) total_units += x.units[0].size();
-    const size_t need_bytes = total_units * sizeof(Unit) + (size_t)(s->sm_count + 1) * sizeof(int);
+    const size_t need_bytes = total_units * sizeof(Unit) + (size_t)(s->sm_count + 1) * sizeof(int) +
+                              16 + (size_t)s->max_channels * sizeof(FrameCopy);
     if (need_bytes > s->slot_cap) {
         const size_t cap = std::max(need_bytes, s->slot_cap * 2);
         e = cudaDeviceSynchronize();
@@ -333,7 +361,14 @@ int chx_stream_frame_slot(chx_stream *s, int channel_id, uint8_t **d_slot) {
 int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const *d_frames,
                       const int64_t *arrival_ns, void *stream) {
     clear_error();
-    if (!s || (n > 0 && !ids)) return fail(CHX_E_INVALID, "NULL argument");
+    if (!s || n < 0 || (n > 0 && !ids)) return fail(CHX_E_INVALID, "NULL argument");
+    // Validate everything before any channel state moves.
+    for (int i = 0; i < n; i++) {
+        if (ids[i] < 0 || ids[i] >= (int)s->chans.size())
+            return fail(CHX_E_INVALID, "channel id %d", ids[i]);
+        if (d_frames && d_frames[i] && (reinterpret_cast<uintptr_t>(d_frames[i]) & 15))
+            return fail(CHX_E_INVALID, "frame %d is not 16-byte aligned", i);
+    }
     DeviceGuard g(s->device);
     cudaStream_t st = (cudaStream_t)stream;
     Pending *pend = nullptr;
@@ -360,23 +395,13 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
         s->spare.push_back(p);
     };
     std::vector<Unit> units;
+    std::vector<FrameCopy> copies;
     for (int i = 0; i < n; i++) {
         const int id = ids[i];
-        if (id < 0 || id >= (int)s->chans.size()) {
-            drop(pend);
-            return fail(CHX_E_INVALID, "channel id %d", id);
-        }
         StreamChan &c = s->chans[id];
         uint8_t *slot = c.ring + ((int64_t)c.half * c.TA + c.filled) * c.E;
         const uint8_t *src = d_frames ? d_frames[i] : nullptr;
-        if (src && src != slot) {
-            const cudaError_t e = cudaMemcpyAsync(slot, src, (size_t)s->frame_len * c.E,
-                                                  cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) {
-                drop(pend);
-                return cuda_fail(e, "frame copy");
-            }
-        }
+        if (src && src != slot) copies.push_back({src, slot, (int64_t)s->frame_len * c.E});
         c.filled += s->frame_len;
         c.last_arrival = arrival_ns ? arrival_ns[i] : now_ns();
         s->frames++;
@@ -388,16 +413,18 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
             c.filled = 0;
         }
     }
-    if (units.empty()) {
+    if (units.empty() && copies.empty()) {
         drop(pend);
         return CHX_OK;
     }
     const int slots = std::max(1, s->sm_count / 2);
-    const int grid = (int)std::min<size_t>(units.size(), (size_t)slots);
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>(units.size(), (size_t)slots));
     std::vector<int> offsets;
-    tc_schedule(units, grid, offsets);
+    if (!units.empty()) tc_schedule(units, grid, offsets);
+    // Slot table: units, then grid + 1 offsets, then the frame copies (16-byte aligned).
     const size_t ub = units.size() * sizeof(Unit);
-    const size_t tb = ub + offsets.size() * sizeof(int);
+    const size_t cb0 = (ub + offsets.size() * sizeof(int) + 15) / 16 * 16;
+    const size_t tb = cb0 + copies.size() * sizeof(FrameCopy);
     if (tb > s->slot_cap) {
         drop(pend);
         return fail(CHX_E_INVALID, "unit table overflow");
@@ -409,30 +436,40 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     if (e == cudaSuccess) {
         memcpy(sl.host, units.data(), ub);
         memcpy((char *)sl.host + ub, offsets.data(), offsets.size() * sizeof(int));
+        memcpy((char *)sl.host + cb0, copies.data(), copies.size() * sizeof(FrameCopy));
         e = cudaMemcpyAsync(sl.dev, sl.host, tb, cudaMemcpyHostToDevice, st);
     }
-    if (e != cudaSuccess) {
-        drop(pend);
-        return cuda_fail(e, "unit table upload");
+    if (e == cudaSuccess && !copies.empty())
+        e = launch_frame_copies((const FrameCopy *)((const char *)sl.dev + cb0), (int)copies.size(),
+                                st);
+    if (e == cudaSuccess && !units.empty()) {
+        TcLaunch L;
+        L.chans = s->d_chans;
+        L.units = (const Unit *)sl.dev;
+        L.nunits = (int)units.size();
+        L.cta_offsets = (const int *)((const char *)sl.dev + ub);
+        L.out_base = 0;
+        L.use_param_map = 0;
+        L.map = MAP_EXACT;
+        L.ut = s->ut;
+        L.accumulate = 0;
+        L.err = s->d_err;
+        L.grid = grid;
+        e = tc_pair_launch(L, nullptr, nullptr, st);
     }
-    TcLaunch L;
-    L.chans = s->d_chans;
-    L.units = (const Unit *)sl.dev;
-    L.nunits = (int)units.size();
-    L.cta_offsets = (const int *)((const char *)sl.dev + ub);
-    L.out_base = 0;
-    L.use_param_map = 0;
-    L.map = MAP_EXACT;
-    L.ut = s->ut;
-    L.accumulate = 0;
-    L.err = s->d_err;
-    L.grid = grid;
-    e = tc_pair_launch(L, nullptr, nullptr, st);
     if (e == cudaSuccess) e = cudaEventRecord(sl.done, st);
-    if (e == cudaSuccess) e = cudaEventRecord(pend->ev, st);
     if (e != cudaSuccess) {
         drop(pend);
         return cuda_fail(e, "stream launch");
+    }
+    if (pend->items.empty()) {  // frames copied, no integration completed
+        drop(pend);
+        return CHX_OK;
+    }
+    e = cudaEventRecord(pend->ev, st);
+    if (e != cudaSuccess) {
+        drop(pend);
+        return cuda_fail(e, "completion event");
     }
     {
         std::lock_guard<std::mutex> lock(s->mu);
