@@ -38,6 +38,18 @@ def vis_ops(E, T, F):
     return OPS_PER_VIS_SAMPLE * E * (E + 1) / 2 * T * F
 
 
+def max_over_ranks(value, dist, device):
+    """The maximum of `value` over all ranks (the job's time is the slowest
+    rank's); `value` itself when there is no process group.  `device` is where
+    the collective's tensor lives (the rank's GPU for NCCL, CPU for gloo)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def env_rank():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
             int(os.environ.get("WORLD_SIZE", 1)))
@@ -197,7 +209,7 @@ def run_reference_arm(args):
                           "oracle/_ref/cpu_corr_ref not built (needs the reference sources)"}))
         return 0
     cores = os.cpu_count() or 1
-    t_sample = 384  # per process per step: E=2048 x 384 samples, ~2 s of CPU work per core
+    t_sample = args.ref_sample  # per process per step (384: ~2 s of CPU work per core)
     for _ in range(args.warmup):
         cpu_reference_rate(E, 8, max_procs=cores)
     rates, walls = [], []
@@ -278,10 +290,7 @@ def run_plain(args, torch, cx, dist):
     plan.check_device()
     total_ms = t_start.elapsed_time(t_end)
     per_launch = [a.elapsed_time(b) for a, b in ev]
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     value = ops_step * world * args.steps / (total_ms * 1e-3) / 1e12
     clocks = clk.summary()
 
@@ -390,10 +399,7 @@ def run_e2e(args, torch, cx, plan, dev, ops_step, world, dist):
     t1.record(d2h)
     torch.cuda.synchronize(dev)
     ms = t0.elapsed_time(t1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     return {"value": ops_step * world * steps / (ms * 1e-3) / 1e12, "unit": "TOPS",
             "h2d_bytes_per_step": nin, "d2h_bytes_per_step": nout * 4,
             "ms_per_step": ms / steps, "steps": steps,
@@ -415,6 +421,8 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="tensor-core tile: 0 auto, 1 one SM, 2 SM pair")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=384,
+                    help="reference arm: samples per process per step")
     ap.add_argument("--no-tune", action="store_true",
                     help="batched: skip the autotuner (default tiles; profiling cases)")
     ap.add_argument("--no-plain", action="store_true",

@@ -90,10 +90,7 @@ def run_batched(args, torch, cx, dist):
         b.record(stream)
         torch.cuda.synchronize(dev)
         ms = a.elapsed_time(b)
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item()) / steps
+        return B.max_over_ranks(ms, dist, dev) / steps
 
     steps = args.steps
     with B.ClockSampler(local_rank) as clk:
@@ -228,10 +225,7 @@ def run_stream(args, torch, cx, dist):
         clk.mark_end()
     ms = a.elapsed_time(b)
     s.check_device()
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item())
+    ms = B.max_over_ranks(ms, dist, dev)
     dumps_flat = s.stats()["dumps"] - launches0
     sps = ticks * frame / (ms * 1e-3)        # samples/s per channel sustained
     rt_channels = n * sps / B.REALTIME_SPS     # channels of this mix in real time

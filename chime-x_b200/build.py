@@ -69,7 +69,7 @@ def build(clean=False, verbose=False):
     host_src = os.path.join(HERE, "host", "correlator_test.c")
     if os.path.exists(host_src) and _newer([host_src, LIB, os.path.join(ROOT, "include", "chimex.h")], HOST_BIN):
         cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-        _run(["gcc", "-O2", "-std=gnu99", "-Wall", "-I", os.path.join(ROOT, "include"),
+        _run(["gcc", "-O2", "-std=gnu99", "-Wall", "-fopenmp", "-I", os.path.join(ROOT, "include"),
               "-I", os.path.join(cuda_home, "include"), "-o", HOST_BIN, host_src,
               "-L", HERE, "-lchimex", "-L", os.path.join(cuda_home, "lib64"), "-lcudart",
               "-Wl,-rpath,$ORIGIN", "-lm"])
