@@ -149,7 +149,7 @@ int chx_blocks_to_full(chx_plan *plan, const int32_t *d_blocks, int32_t *d_full,
  * This entry point computes exactly what chx_correlate computes for a plan
  * of (E, F, T, upper_triangle_convention), needs no plan and calls no
  * allocator: its work tables live in a fixed-size array inside the library
- * (about 144 KiB on every GPU that loads it, kept until exit).  Limits: F <= 64 channels and at
+ * (about 162 KiB on every GPU that loads it, kept until exit).  Limits: F <= 64 channels and at
  * most 4096 work units (72 per E=2048 channel per 262144 samples); larger
  * calls return CHX_E_UNSUPPORTED.  The first call on each device looks the
  * array up (and so loads the library's device code); make that first call
