@@ -483,7 +483,15 @@ cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, const CUtenso
 
 }  // namespace
 
-int tc_default_tile(int E) { return E >= 512 ? kTile2Sm : kTile1Sm; }
+// The SM-pair kernel's 256-element units cover an odd number of 128-element
+// tiles with a half-empty row and column of units; measured on B200 (F x
+// T = 16 x 16384) it wins for every even tile count (E = 256: 1150 vs 1040
+// TOPS, 2048: 2416 vs 2200) and loses for every odd one (E = 640: 918 vs 1613,
+// 1920: 2130 vs 2171).
+int tc_default_tile(int E) {
+    const int nt = (E + 127) / 128;
+    return (nt % 2 == 0) ? kTile2Sm : kTile1Sm;
+}
 
 bool tc_supported(int E, int T) { return E >= 32 && E % 32 == 0 && E <= 65536 && T >= 1; }
 

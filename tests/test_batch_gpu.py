@@ -51,8 +51,9 @@ def run_batch(cx, specs, ut=1, seed=7):
 @pytest.mark.gpu
 @pytest.mark.parametrize("ut", [0, 1])
 def test_ragged_batch_small_tile(chimex, ut):
-    # all E < 512: the one-SM tile by default
-    specs = [(96, 77, 2, 128), (160, 128, 1, 0), (256, 300, 3, 0), (32, 33, 1, 48),
+    # the costliest channel (E=384) spans 3 tiles of 128, an odd count: the
+    # one-SM tile for every channel
+    specs = [(96, 77, 2, 128), (160, 128, 1, 0), (384, 300, 3, 0), (32, 33, 1, 48),
              (64, 1, 2, 0), (224, 95, 2, 256)]
     b, chans, hosts = run_batch(chimex, specs, ut)
     b.run(accumulate=False)
@@ -70,7 +71,8 @@ def test_ragged_batch_small_tile(chimex, ut):
 
 @pytest.mark.gpu
 def test_ragged_batch_pair_tile(chimex):
-    # the heaviest channel has E >= 512: the SM-pair tile for every channel
+    # the costliest channel (E=512) spans 4 tiles of 128, an even count: the
+    # SM-pair tile for every channel
     specs = [(512, 200, 2, 0), (96, 77, 1, 0), (288, 64, 3, 320), (640, 129, 1, 0)]
     b, chans, hosts = run_batch(chimex, specs, 1, seed=11)
     b.run()
