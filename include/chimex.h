@@ -60,7 +60,8 @@ extern "C" {
 /* Plan options. */
 #define CHX_OPT_ALGO 1      /* one of CHX_ALGO_* */
 #define CHX_OPT_TSPLIT 2    /* number of sample-range splits (0 = auto) */
-#define CHX_OPT_TILE 3      /* tensor-core tile variant: 0 auto, 1 one SM
+#define CHX_OPT_TILE 3      /* tensor-core tile variant: 0 auto (SM pair when
+                               ceil(E/128) is even, else one SM), 1 one SM
                                (128 x 256 elements), 2 SM pair (256 x 256) */
 
 typedef struct chx_plan chx_plan;
@@ -97,7 +98,9 @@ int64_t chx_plan_triangle_words(const chx_plan *plan);
 /* Fused correlator: exact visibilities of d_packed written into d_blocks in
  * the reference block layout.  accumulate = 0 overwrites d_blocks, 1 adds
  * to it.  Replaces the offsetAccumulateElements -> preseed -> corr chain of
- * main_wrapper.c:693-777 (whose net result is the same buffer). */
+ * main_wrapper.c:693-777 (whose net result is the same buffer).  The
+ * tensor-core path needs d_packed and d_blocks 16-byte aligned (TMA) and
+ * returns CHX_E_INVALID otherwise. */
 int chx_correlate(chx_plan *plan, const uint8_t *d_packed, int32_t *d_blocks,
                   void *stream, int accumulate);
 
