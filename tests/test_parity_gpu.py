@@ -236,3 +236,25 @@ def test_tc_repeatable_against_simt(chimex, E, F, T):
             p.correlate(d, out)
             p.check_device()
             assert torch.equal(out, ref), algo
+
+
+def test_tensor_core_path_rejects_unaligned_buffers(chimex):
+    """TMA needs 16-byte aligned input and block buffers: an unaligned pointer is
+    refused with CHX_E_INVALID before anything is enqueued."""
+    import ctypes
+    cx = chimex
+    E, F, T = 256, 1, 64
+    p = make_plan(cx, E, F, T, algo="tc2")
+    x = torch.zeros(p.input_bytes + 64, dtype=torch.uint8, device="cuda")
+    y = torch.zeros(p.block_words + 16, dtype=torch.int32, device="cuda")
+    lib = cx.lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    h = p._h
+    assert lib.chx_correlate(h, ctypes.c_void_p(x.data_ptr() + 4), ctypes.c_void_p(y.data_ptr()),
+                             s, 0) == cx.E_INVALID
+    assert lib.chx_correlate(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr() + 4),
+                             s, 0) == cx.E_INVALID
+    assert "aligned" in lib.chx_last_error().decode()
+    assert lib.chx_correlate(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
+                             s, 0) == cx.OK
+    p.check_device()
