@@ -32,6 +32,12 @@ using namespace chx;
 
 namespace {
 
+// Device buffers passed to the plan entry points must be 16-byte aligned: the
+// tensor-core kernels move them with TMA and the CUDA-core kernels with 8-
+// and 16-byte vector accesses.  (Allocations from cudaMalloc and torch are
+// 256-byte aligned.)
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 void free_plan_device(chx_plan *p) {
     if (p->d_err) cudaFree(p->d_err);
     if (p->d_chans) cudaFree(p->d_chans);
@@ -250,6 +256,8 @@ int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void 
                   int accumulate) {
     clear_error();
     if (!p || !d_packed || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
+    if (!aligned16(d_packed) || !aligned16(d_blocks))
+        return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
     DeviceGuard g(p->device);
     cudaStream_t st = (cudaStream_t)stream;
     const bool use_tc =
@@ -274,6 +282,8 @@ int chx_offset_accumulate(chx_plan *p, const uint8_t *d_packed, uint32_t *d_sums
                           void *stream, int accumulate) {
     clear_error();
     if (!p || !d_packed || !d_sums) return fail(CHX_E_INVALID, "NULL argument");
+    if (!aligned16(d_packed) || !aligned16(d_sums))
+        return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
     DeviceGuard g(p->device);
     cudaStream_t st = (cudaStream_t)stream;
     if (!accumulate)
@@ -285,6 +295,8 @@ int chx_offset_accumulate(chx_plan *p, const uint8_t *d_packed, uint32_t *d_sums
 int chx_preseed(chx_plan *p, const uint32_t *d_sums, int32_t *d_blocks, void *stream) {
     clear_error();
     if (!p || !d_sums || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
+    if (!aligned16(d_sums) || !aligned16(d_blocks))
+        return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
     DeviceGuard g(p->device);
     CHX_CUDA(launch_preseed(d_sums, d_blocks, p->E, p->F, p->T, p->kernel_batch, p->ut,
                             (cudaStream_t)stream));
@@ -294,6 +306,8 @@ int chx_preseed(chx_plan *p, const uint32_t *d_sums, int32_t *d_blocks, void *st
 int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void *stream) {
     clear_error();
     if (!p || !d_packed || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
+    if (!aligned16(d_packed) || !aligned16(d_blocks))
+        return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
     // The reference kernels' own domain (main_wrapper.c:564-569,
     // pairwise_correlator_UT.cl:82, help text main_wrapper.c:57).
     if (p->T % p->TA != 0)
@@ -323,6 +337,8 @@ int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, voi
 int chx_blocks_to_triangle(chx_plan *p, const int32_t *d_blocks, int32_t *d_tri, void *stream) {
     clear_error();
     if (!p || !d_blocks || !d_tri) return fail(CHX_E_INVALID, "NULL argument");
+    if (!aligned16(d_blocks) || !aligned16(d_tri))
+        return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
     DeviceGuard g(p->device);
     CHX_CUDA(launch_blocks_to_triangle(d_blocks, d_tri, p->E, p->F, (cudaStream_t)stream));
     return CHX_OK;
@@ -331,6 +347,8 @@ int chx_blocks_to_triangle(chx_plan *p, const int32_t *d_blocks, int32_t *d_tri,
 int chx_blocks_to_full(chx_plan *p, const int32_t *d_blocks, int32_t *d_full, void *stream) {
     clear_error();
     if (!p || !d_blocks || !d_full) return fail(CHX_E_INVALID, "NULL argument");
+    if (!aligned16(d_blocks) || !aligned16(d_full))
+        return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
     DeviceGuard g(p->device);
     CHX_CUDA(launch_blocks_to_full(d_blocks, d_full, p->E, p->F, (cudaStream_t)stream));
     return CHX_OK;

@@ -23,7 +23,9 @@
  *
  * Conventions: every function returns CHX_OK (0) or a negative CHX_E_* code
  * and sets a thread-local message readable with chx_last_error().  Device
- * pointers and streams are owned by the caller; the library owns its plans,
+ * pointers must be 16-byte aligned (TMA and vector accesses; cudaMalloc and
+ * torch allocations are 256-byte aligned) and are refused with CHX_E_INVALID
+ * otherwise.  Device pointers and streams are owned by the caller; the library owns its plans,
  * their small device-side tables and any scratch a plan allocates at
  * creation.  Work is enqueued asynchronously on the given stream (a
  * cudaStream_t passed as void*; NULL = the legacy default stream).  A plan is

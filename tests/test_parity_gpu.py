@@ -258,3 +258,15 @@ def test_tensor_core_path_rejects_unaligned_buffers(chimex):
     assert lib.chx_correlate(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr()),
                              s, 0) == cx.OK
     p.check_device()
+    # the CUDA-core path and the helper kernels refuse them too
+    p.set_option(cx.OPT_ALGO, cx.ALGO_SIMT)
+    assert lib.chx_correlate(h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(y.data_ptr() + 8),
+                             s, 0) == cx.E_INVALID
+    sums = torch.zeros(p.sum_words + 8, dtype=torch.int32, device="cuda")
+    assert lib.chx_offset_accumulate(h, ctypes.c_void_p(x.data_ptr() + 4),
+                                     ctypes.c_void_p(sums.data_ptr()), s, 0) == cx.E_INVALID
+    assert lib.chx_preseed(h, ctypes.c_void_p(sums.data_ptr() + 4), ctypes.c_void_p(y.data_ptr()),
+                           s) == cx.E_INVALID
+    tri = torch.zeros(p.triangle_words + 8, dtype=torch.int32, device="cuda")
+    assert lib.chx_blocks_to_triangle(h, ctypes.c_void_p(y.data_ptr()),
+                                      ctypes.c_void_p(tri.data_ptr() + 8), s) == cx.E_INVALID
