@@ -63,6 +63,7 @@ _sig("chx_blocks_to_triangle", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_blocks_to_full", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_plan_check", _i, [_vp, _vp])
 _sig("chx_correlate_noalloc", _i, [_vp, _vp, _i, _i, _i, _i, _i, _vp])
+_sig("chx_selftest_bounded_wait", _i, [_i, _i, ctypes.POINTER(_i)])
 
 
 class ChannelDesc(ctypes.Structure):
@@ -103,7 +104,7 @@ EXPORTED = [
     "chx_plan_set_option", "chx_plan_block_words", "chx_plan_input_bytes",
     "chx_plan_sum_words", "chx_plan_triangle_words", "chx_correlate",
     "chx_offset_accumulate", "chx_preseed", "chx_corr_compat", "chx_blocks_to_triangle",
-    "chx_blocks_to_full", "chx_plan_check", "chx_correlate_noalloc",
+    "chx_blocks_to_full", "chx_plan_check", "chx_correlate_noalloc", "chx_selftest_bounded_wait",
     "chx_batch_create", "chx_batch_run", "chx_batch_work_units", "chx_batch_ops",
     "chx_batch_check", "chx_batch_destroy", "chx_autotune", "chx_stream_create",
     "chx_stream_admit", "chx_stream_frame_slot", "chx_stream_submit", "chx_stream_last_dump",
@@ -150,6 +151,14 @@ def device_view(addr, n, dtype="int32", device=0):
     import torch
     ts = {"int32": "<i4", "uint8": "|u1", "uint32": "<u4"}[dtype]
     return torch.as_tensor(_DeviceArray(addr, n, ts), device=torch.device("cuda", device))
+
+
+def selftest_bounded_wait(mode=0, device=0):
+    """Runs the bounded-wait self-test (chx_selftest_bounded_wait); returns
+    (status code, elapsed ms).  CHX_E_TIMEOUT is the expected status."""
+    ms = _i()
+    code = _lib.chx_selftest_bounded_wait(device, mode, ctypes.byref(ms))
+    return code, ms.value
 
 
 def num_blocks(E):

@@ -143,6 +143,7 @@ const char *chx_last_error(void) { return g_err; }
 int chx_plan_create(chx_plan **plan, int E, int F, int T, int TA, int ut, int kernel_batch,
                     int device) {
     clear_error();
+    NvtxRange nvtx_("chx_plan_create");
     if (!plan) return fail(CHX_E_INVALID, "plan pointer is NULL");
     *plan = nullptr;
     if (E < 32 || E % 32 != 0)
@@ -255,6 +256,7 @@ static int auto_splits(int64_t units, int T, int sm_count, int min_chunk) {
 int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void *stream,
                   int accumulate) {
     clear_error();
+    NvtxRange nvtx_("chx_correlate");
     if (!p || !d_packed || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
     if (!aligned16(d_packed) || !aligned16(d_blocks))
         return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
@@ -281,6 +283,7 @@ int chx_correlate(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void 
 int chx_offset_accumulate(chx_plan *p, const uint8_t *d_packed, uint32_t *d_sums,
                           void *stream, int accumulate) {
     clear_error();
+    NvtxRange nvtx_("chx_offset_accumulate");
     if (!p || !d_packed || !d_sums) return fail(CHX_E_INVALID, "NULL argument");
     if (!aligned16(d_packed) || !aligned16(d_sums))
         return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
@@ -294,6 +297,7 @@ int chx_offset_accumulate(chx_plan *p, const uint8_t *d_packed, uint32_t *d_sums
 
 int chx_preseed(chx_plan *p, const uint32_t *d_sums, int32_t *d_blocks, void *stream) {
     clear_error();
+    NvtxRange nvtx_("chx_preseed");
     if (!p || !d_sums || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
     if (!aligned16(d_sums) || !aligned16(d_blocks))
         return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
@@ -305,6 +309,7 @@ int chx_preseed(chx_plan *p, const uint32_t *d_sums, int32_t *d_blocks, void *st
 
 int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, void *stream) {
     clear_error();
+    NvtxRange nvtx_("chx_corr_compat");
     if (!p || !d_packed || !d_blocks) return fail(CHX_E_INVALID, "NULL argument");
     if (!aligned16(d_packed) || !aligned16(d_blocks))
         return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
@@ -336,6 +341,7 @@ int chx_corr_compat(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, voi
 
 int chx_blocks_to_triangle(chx_plan *p, const int32_t *d_blocks, int32_t *d_tri, void *stream) {
     clear_error();
+    NvtxRange nvtx_("chx_blocks_to_triangle");
     if (!p || !d_blocks || !d_tri) return fail(CHX_E_INVALID, "NULL argument");
     if (!aligned16(d_blocks) || !aligned16(d_tri))
         return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");
@@ -346,6 +352,7 @@ int chx_blocks_to_triangle(chx_plan *p, const int32_t *d_blocks, int32_t *d_tri,
 
 int chx_blocks_to_full(chx_plan *p, const int32_t *d_blocks, int32_t *d_full, void *stream) {
     clear_error();
+    NvtxRange nvtx_("chx_blocks_to_full");
     if (!p || !d_blocks || !d_full) return fail(CHX_E_INVALID, "NULL argument");
     if (!aligned16(d_blocks) || !aligned16(d_full))
         return fail(CHX_E_INVALID, "device buffers must be 16-byte aligned");

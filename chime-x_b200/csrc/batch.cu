@@ -117,6 +117,7 @@ extern "C" {
 
 int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int ut, int device) {
     clear_error();
+    NvtxRange nvtx_("chx_batch_create");
     if (!out || !descs || n < 1) return fail(CHX_E_INVALID, "need at least one channel");
     *out = nullptr;
     if (ut != 0 && ut != 1) return fail(CHX_E_INVALID, "upper_triangle_convention=%d", ut);
@@ -269,6 +270,7 @@ int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int 
 
 int chx_batch_run(chx_batch *b, void *stream, int accumulate) {
     clear_error();
+    NvtxRange nvtx_("chx_batch_run");
     if (!b) return fail(CHX_E_INVALID, "batch is NULL");
     DeviceGuard g(b->device);
     CHX_CUDA(cudaGraphLaunch(b->exec[accumulate ? 1 : 0], (cudaStream_t)stream));
@@ -307,6 +309,7 @@ int chx_batch_check(chx_batch *b, void *stream) {
 int chx_autotune(int E, int T, const uint8_t *d_in, int32_t *d_out, void *stream, int *best_tile,
                  int *best_split, double *best_ms) {
     clear_error();
+    NvtxRange nvtx_("chx_autotune");
     if (!d_in || !d_out) return fail(CHX_E_INVALID, "NULL scratch buffer");
     int dev = 0;
     CHX_CUDA(cudaGetDevice(&dev));

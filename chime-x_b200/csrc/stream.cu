@@ -253,6 +253,7 @@ int chx_stream_create(chx_stream **out, int max_channels, int frame_len, int ut,
 
 int chx_stream_admit(chx_stream *s, int E, int TA, int *channel_id) {
     clear_error();
+    NvtxRange nvtx_("chx_stream_admit");
     if (!s || !channel_id) return fail(CHX_E_INVALID, "NULL argument");
     if ((int)s->chans.size() >= s->max_channels)
         return fail(CHX_E_ADMISSION, "stream already holds %d channels", s->max_channels);
@@ -361,6 +362,7 @@ int chx_stream_frame_slot(chx_stream *s, int channel_id, uint8_t **d_slot) {
 int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const *d_frames,
                       const int64_t *arrival_ns, void *stream) {
     clear_error();
+    NvtxRange nvtx_("chx_stream_submit");
     if (!s || n < 0 || (n > 0 && !ids)) return fail(CHX_E_INVALID, "NULL argument");
     // Validate everything before any channel state moves.
     for (int i = 0; i < n; i++) {

@@ -169,6 +169,16 @@ int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks, int num_el
  * Synchronises the stream.  Returns CHX_OK or CHX_E_TIMEOUT. */
 int chx_plan_check(chx_plan *plan, void *stream);
 
+/* Self-test of the bounded device-side waits (no counterpart in the
+ * reference, whose kernels spin without a bound).  Runs one CTA on `device`
+ * that waits, with the same helper and 2 s limit as the correlator kernels,
+ * on a barrier phase that nothing completes: mode 0 lets the limit run out,
+ * mode 1 raises the CTA's abort flag after ~10 ms.  Returns CHX_E_TIMEOUT when
+ * the wait gave up as designed (elapsed_ms: how long it waited), CHX_E_INVALID
+ * if it claimed completion, CHX_E_CUDA on a CUDA error.  The context stays
+ * usable afterwards. */
+int chx_selftest_bounded_wait(int device, int mode, int *elapsed_ms);
+
 /* ---------------------------------------------------------------------
  * Batched ragged launch: many channels with their own element counts and
  * sample counts in one persistent launch (captured in a CUDA graph).
