@@ -61,12 +61,20 @@ cudaError_t build_tc_tables(chx_plan *p) {
         chans[f].orow = (int)((int64_t)f * p->NB * 32);
     }
     std::vector<Unit> units;
-    const int tile = p->tile ? p->tile : tc_default_tile(p->E);
+    // Unset options take the autotuner's cached choice for this shape, if any,
+    // else the default tile and no split.
+    int tile = p->tile, split = p->tsplit;
+    int tuned_tile = 0, tuned_split = 0;
+    if ((!tile || !split) && tc_tune_lookup(p->device, p->E, p->T, &tuned_tile, &tuned_split)) {
+        if (!tile) tile = tuned_tile;
+        if (!split) split = tuned_split;
+    }
+    if (!tile) tile = tc_default_tile(p->E);
     for (int f = 0; f < p->F; f++) {
         if (tile == kTile2Sm)
-            tc_append_pair_units(units, f, p->E, 0, p->T, p->tsplit, 0);
+            tc_append_pair_units(units, f, p->E, 0, p->T, split, 0);
         else
-            tc_append_units(units, f, p->E, 0, p->T, p->tsplit, 0);
+            tc_append_units(units, f, p->E, 0, p->T, split, 0);
     }
     const int slots = tile == kTile2Sm ? p->sm_count / 2 : p->sm_count;
     const int grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, slots));

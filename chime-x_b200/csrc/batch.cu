@@ -55,6 +55,15 @@ bool tune_lookup(int device, int E, int T, TuneVal *out) {
 }
 
 }  // namespace
+
+bool tc_tune_lookup(int device, int E, int T, int *tile, int *split) {
+    TuneVal tv;
+    if (!tune_lookup(device, E, T, &tv)) return false;
+    *tile = tv.tile;
+    *split = tv.split;
+    return true;
+}
+
 }  // namespace chx
 
 struct chx_batch {

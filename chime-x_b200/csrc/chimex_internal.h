@@ -185,5 +185,9 @@ cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map,
 constexpr int kTile1Sm = 1;  // 128 x 256 elements per CTA
 constexpr int kTile2Sm = 2;  // 256 x 256 elements per CTA pair
 int tc_default_tile(int E);
+// The autotuner's cached choice for (device, E, T) (batch.cu): true and the
+// tile variant and split count when an entry with the same E and a T within a
+// factor 2 exists.
+bool tc_tune_lookup(int device, int E, int T, int *tile, int *split);
 
 }  // namespace chx

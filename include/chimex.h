@@ -210,7 +210,9 @@ int chx_batch_check(chx_batch *batch, void *stream);
 int chx_batch_destroy(chx_batch *batch);
 
 /* Times the tensor-core tile variants and split counts for (E, T) on the
- * current device and caches the winner for chx_batch_create / AUTO plans.
+ * current device and caches the winner: batches and plans created afterwards
+ * (with CHX_OPT_TILE / CHX_OPT_TSPLIT left at 0) take it for channels of the
+ * same E and a T within a factor 2.
  * d_scratch_in/d_scratch_out must hold T*E bytes and NB*2048 int32. */
 int chx_autotune(int num_elements, int num_timesamples, const uint8_t *d_scratch_in,
                  int32_t *d_scratch_out, void *stream, int *best_tile,

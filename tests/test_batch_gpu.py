@@ -181,7 +181,12 @@ def test_autotune_choice_is_exact(chimex):
     b.check_device()
     p = cx.Plan(E, 1, T, T)
     p.set_option(cx.OPT_ALGO, cx.ALGO_SIMT)
-    assert torch.equal(blocks, p.correlate(x))
+    ref = p.correlate(x)
+    assert torch.equal(blocks, ref)
+    # a plan of this shape created now takes the tuned tile and split too
+    q = cx.Plan(E, 1, T, T)
+    assert torch.equal(q.correlate(x), ref)
+    q.check_device()
 
 
 def test_batch_validation_without_device():
