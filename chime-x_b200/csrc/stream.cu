@@ -10,7 +10,9 @@
 // Each submit appends one frame per listed channel to its ring (in place when
 // the caller wrote it into the slot returned by chx_stream_frame_slot).  The
 // channels whose integration completes are correlated by one persistent
-// tensor-core launch over all their work units: the integration's samples
+// tensor-core launch over all their work units (two launches when channels of
+// both tile variants complete: SM pair for an even 128-element tile count,
+// one SM for an odd one): the integration's samples
 // accumulate in TMEM and each dump buffer is written once, so the resident
 // state never travels through HBM per frame.  An event recorded after each
 // launch is watched by the stream's completion thread, which records, per
@@ -44,6 +46,7 @@ struct StreamChan {
     uint8_t *ring = nullptr;     // [2][TA][E]
     int32_t *dumps = nullptr;    // [2][NB][2048]
     std::vector<Unit> units[2];  // work of ring half h -> dump h
+    bool pair = true;            // units for the SM-pair kernel (else the one-SM kernel)
     int half = 0;                // half being filled
     int filled = 0;              // samples in that half
     int64_t seq = 0;             // integrations completed (dispatched)
@@ -270,8 +273,15 @@ int chx_stream_admit(chx_stream *s, int E, int TA, int *channel_id) {
     // units: both halves of this channel
     std::vector<Unit> u0, u1;
     const int cid = (int)s->chans.size();
-    tc_append_pair_units(u0, cid, E, 0, TA, 1, 0);
-    tc_append_pair_units(u1, cid, E, TA, 2 * TA, 1, NB * 2048);
+    // The tile variant the plain path would choose for this E.
+    const bool pair = tc_default_tile(E) == kTile2Sm;
+    if (pair) {
+        tc_append_pair_units(u0, cid, E, 0, TA, 1, 0);
+        tc_append_pair_units(u1, cid, E, TA, 2 * TA, 1, NB * 2048);
+    } else {
+        tc_append_units(u0, cid, E, 0, TA, 1, 0);
+        tc_append_units(u1, cid, E, TA, 2 * TA, 1, NB * 2048);
+    }
     const int64_t need = ring_bytes + dump_bytes;
     if (s->budget > 0) {
         if (s->resident + need > s->budget)
@@ -319,12 +329,14 @@ int chx_stream_admit(chx_stream *s, int E, int TA, int *channel_id) {
     CHX_CUDA(cudaMemcpy(s->d_chans + cid, &d, sizeof(ChanDesc), cudaMemcpyHostToDevice));
     c.units[0] = std::move(u0);
     c.units[1] = std::move(u1);
+    c.pair = pair;
     // Grow the per-launch unit tables to hold every channel completing at
     // once.  Growing waits for all launches that read the old tables.
     size_t total_units = c.units[0].size();
     for (const auto &x : s->chans) total_units += x.units[0].size();
-    const size_t need_bytes = total_units * sizeof(Unit) + (size_t)(s->sm_count + 1) * sizeof(int) +
-                              16 + (size_t)s->max_channels * sizeof(FrameCopy);
+    const size_t need_bytes = total_units * sizeof(Unit) +
+                              2 * ((size_t)(s->sm_count + 1) * sizeof(int) + 16) +
+                              (size_t)s->max_channels * sizeof(FrameCopy);
     if (need_bytes > s->slot_cap) {
         const size_t cap = std::max(need_bytes, s->slot_cap * 2);
         e = cudaDeviceSynchronize();
@@ -396,7 +408,7 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
         std::lock_guard<std::mutex> lock(s->mu);
         s->spare.push_back(p);
     };
-    std::vector<Unit> units;
+    std::vector<Unit> units, units1;  // SM-pair and one-SM kernel work
     std::vector<FrameCopy> copies;
     for (int i = 0; i < n; i++) {
         const int id = ids[i];
@@ -408,24 +420,34 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
         c.last_arrival = arrival_ns ? arrival_ns[i] : now_ns();
         s->frames++;
         if (c.filled == c.TA) {
-            units.insert(units.end(), c.units[c.half].begin(), c.units[c.half].end());
+            std::vector<Unit> &dst = c.pair ? units : units1;
+            dst.insert(dst.end(), c.units[c.half].begin(), c.units[c.half].end());
             pend->items.push_back({id, c.half, c.seq, c.last_arrival});
             c.seq++;
             c.half ^= 1;
             c.filled = 0;
         }
     }
-    if (units.empty() && copies.empty()) {
+    if (units.empty() && units1.empty() && copies.empty()) {
         drop(pend);
         return CHX_OK;
     }
-    const int slots = std::max(1, s->sm_count / 2);
-    const int grid = (int)std::max<size_t>(1, std::min<size_t>(units.size(), (size_t)slots));
-    std::vector<int> offsets;
+    // Each kernel's units go to its own persistent grid (clusters of two CTAs
+    // for the SM-pair kernel, single CTAs for the other).
+    const int grid = (int)std::max<size_t>(
+        1, std::min<size_t>(units.size(), (size_t)std::max(1, s->sm_count / 2)));
+    const int grid1 =
+        (int)std::max<size_t>(1, std::min<size_t>(units1.size(), (size_t)std::max(1, s->sm_count)));
+    std::vector<int> offsets, offsets1;
     if (!units.empty()) tc_schedule(units, grid, offsets);
-    // Slot table: units, then grid + 1 offsets, then the frame copies (16-byte aligned).
+    if (!units1.empty()) tc_schedule(units1, grid1, offsets1);
+    // Slot table: pair units and their offsets, one-SM units and theirs, then
+    // the frame copies; each part 16-byte aligned.
+    auto up16 = [](size_t x) { return (x + 15) / 16 * 16; };
     const size_t ub = units.size() * sizeof(Unit);
-    const size_t cb0 = (ub + offsets.size() * sizeof(int) + 15) / 16 * 16;
+    const size_t u1b0 = up16(ub + offsets.size() * sizeof(int));
+    const size_t u1b = units1.size() * sizeof(Unit);
+    const size_t cb0 = up16(u1b0 + u1b + offsets1.size() * sizeof(int));
     const size_t tb = cb0 + copies.size() * sizeof(FrameCopy);
     if (tb > s->slot_cap) {
         drop(pend);
@@ -436,28 +458,38 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     s->next_slot = (s->next_slot + 1) % kSlots;
     cudaError_t e = cudaEventSynchronize(sl.done);
     if (e == cudaSuccess) {
-        memcpy(sl.host, units.data(), ub);
-        memcpy((char *)sl.host + ub, offsets.data(), offsets.size() * sizeof(int));
-        memcpy((char *)sl.host + cb0, copies.data(), copies.size() * sizeof(FrameCopy));
+        char *h = static_cast<char *>(sl.host);
+        memcpy(h, units.data(), ub);
+        memcpy(h + ub, offsets.data(), offsets.size() * sizeof(int));
+        memcpy(h + u1b0, units1.data(), u1b);
+        memcpy(h + u1b0 + u1b, offsets1.data(), offsets1.size() * sizeof(int));
+        memcpy(h + cb0, copies.data(), copies.size() * sizeof(FrameCopy));
         e = cudaMemcpyAsync(sl.dev, sl.host, tb, cudaMemcpyHostToDevice, st);
     }
     if (e == cudaSuccess && !copies.empty())
         e = launch_frame_copies((const FrameCopy *)((const char *)sl.dev + cb0), (int)copies.size(),
                                 st);
+    TcLaunch L;
+    L.chans = s->d_chans;
+    L.out_base = 0;
+    L.use_param_map = 0;
+    L.map = MAP_EXACT;
+    L.ut = s->ut;
+    L.accumulate = 0;
+    L.err = s->d_err;
     if (e == cudaSuccess && !units.empty()) {
-        TcLaunch L;
-        L.chans = s->d_chans;
         L.units = (const Unit *)sl.dev;
         L.nunits = (int)units.size();
         L.cta_offsets = (const int *)((const char *)sl.dev + ub);
-        L.out_base = 0;
-        L.use_param_map = 0;
-        L.map = MAP_EXACT;
-        L.ut = s->ut;
-        L.accumulate = 0;
-        L.err = s->d_err;
         L.grid = grid;
         e = tc_pair_launch(L, nullptr, nullptr, st);
+    }
+    if (e == cudaSuccess && !units1.empty()) {
+        L.units = (const Unit *)((const char *)sl.dev + u1b0);
+        L.nunits = (int)units1.size();
+        L.cta_offsets = (const int *)((const char *)sl.dev + u1b0 + u1b);
+        L.grid = grid1;
+        e = tc_launch(L, nullptr, nullptr, st);
     }
     if (e == cudaSuccess) e = cudaEventRecord(sl.done, st);
     if (e != cudaSuccess) {
