@@ -209,7 +209,12 @@ def run_reference_arm(args):
                           "oracle/_ref/cpu_corr_ref not built (needs the reference sources)"}))
         return 0
     cores = os.cpu_count() or 1
-    t_sample = args.ref_sample  # per process per step (384: ~2 s of CPU work per core)
+    # Samples per process per step: 384 is ~2 s of CPU work per core; by
+    # default the sample shrinks so that all the timed steps take ~2.5 min.
+    if args.ref_sample:
+        t_sample = args.ref_sample
+    else:
+        t_sample = max(8, min(384, int(384 * (150.0 / max(1, args.steps)) / 2.0)))
     for _ in range(args.warmup):
         cpu_reference_rate(E, 8, max_procs=cores)
     rates, walls = [], []
@@ -421,8 +426,9 @@ def main():
     ap.add_argument("--tile", type=int, default=0, help="tensor-core tile: 0 auto, 1 one SM, 2 SM pair")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-sample", type=int, default=384,
-                    help="reference arm: samples per process per step")
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="reference arm: samples per process per step (0: sized so the "
+                         "timed steps take ~2.5 min)")
     ap.add_argument("--no-tune", action="store_true",
                     help="batched: skip the autotuner (default tiles; profiling cases)")
     ap.add_argument("--no-plain", action="store_true",
