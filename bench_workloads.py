@@ -17,6 +17,7 @@ dump); and the same paced loop end to end, every frame crossing PCIe from
 pinned host memory, for the channels 70% of the measured H2D bandwidth
 carries.
 """
+import gc
 import json
 import time
 
@@ -243,23 +244,30 @@ def run_stream(args, torch, cx, dist):
         s.sync()
         s.reset_stats()
         late = 0
-        t0 = time.monotonic_ns() + 2 * period_ns
-        for k in range(nticks):
-            due = t0 + k * period_ns
-            while True:
-                now = time.monotonic_ns()
-                if now >= due:
-                    break
-                if due - now > 200000:
-                    time.sleep((due - now - 150000) * 1e-9)
-            if now - due > period_ns:
-                late += 1
-            for i in range(len(sel)):
-                arr[i] = due
-            frames = before_submit(k) if before_submit else None
-            s.submit(sel_ids, frames, arr, stream)
-            if after_submit:
-                after_submit(k)
+        # the frame schedule is kept by this Python loop: no garbage
+        # collection pauses inside it
+        gc.collect()
+        gc.disable()
+        try:
+            t0 = time.monotonic_ns() + 2 * period_ns
+            for k in range(nticks):
+                due = t0 + k * period_ns
+                while True:
+                    now = time.monotonic_ns()
+                    if now >= due:
+                        break
+                    if due - now > 200000:
+                        time.sleep((due - now - 150000) * 1e-9)
+                if now - due > period_ns:
+                    late += 1
+                for i in range(len(sel)):
+                    arr[i] = due
+                frames = before_submit(k) if before_submit else None
+                s.submit(sel_ids, frames, arr, stream)
+                if after_submit:
+                    after_submit(k)
+        finally:
+            gc.enable()
         torch.cuda.synchronize(dev)
         s.check_device()
         return s.stats(), late
