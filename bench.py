@@ -8,7 +8,7 @@ MACs per upper-triangle complex visibility per sample; diagonal-tile waste
 not credited).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config plain|batched|stream] [--algo auto|simt|tc]
+                    [--config plain|batched|stream|helpers] [--algo auto|simt|tc]
 
 Under torchrun each rank correlates its own F channels (weak scaling, no
 data-path collective); the time is the max over ranks.  `--impl reference`
@@ -420,7 +420,7 @@ def main():
     ap.add_argument("--F", type=int, default=8, help="channels per GPU (profiling cases)")
     ap.add_argument("--T", type=int, default=16384, help="samples (profiling cases)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="plain", choices=["plain", "batched", "stream"])
+    ap.add_argument("--config", default="plain", choices=["plain", "batched", "stream", "helpers"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "tc"])
     ap.add_argument("--tsplit", type=int, default=0)
     ap.add_argument("--tile", type=int, default=0, help="tensor-core tile: 0 auto, 1 one SM, 2 SM pair")
@@ -456,6 +456,9 @@ def main():
         elif args.config == "batched":
             import bench_workloads
             bench_workloads.run_batched(args, torch, cx, dist)
+        elif args.config == "helpers":
+            import bench_workloads
+            bench_workloads.run_helpers(args, torch, cx, dist)
         else:
             import bench_workloads
             bench_workloads.run_stream(args, torch, cx, dist)

@@ -371,3 +371,59 @@ def run_stream(args, torch, cx, dist):
     s.close()
     if rank == 0:
         print(json.dumps(line))
+
+
+def run_helpers(args, torch, cx, dist):
+    """The HBM-bound kernels of the path on the plain workload (E=2048, F=8,
+    T=16384): offset sums, preseed, block -> triangle and block -> full-matrix
+    reorganisation, each timed with CUDA events over its algorithmic bytes
+    (bytes the kernel must read plus bytes it must write) against the measured
+    HBM copy bandwidth."""
+    rank, local_rank, world = B.env_rank()
+    dev = torch.device("cuda", local_rank)
+    E, F, T = args.E, args.F, args.T
+    p = cx.Plan(E, F, T, 256, 1, 0, local_rank)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(42 + rank)
+    packed = torch.randint(0, 256, (p.input_bytes,), dtype=torch.uint8, device=dev, generator=gen)
+    blocks = p.correlate(packed)
+    sums = torch.empty(p.sum_words, dtype=torch.int32, device=dev)
+    tri = torch.empty(p.triangle_words, dtype=torch.int32, device=dev)
+    full = torch.empty(F * E * E * 2, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    nb_bytes = p.block_words * 4
+    cases = {
+        "offset_accumulate": (lambda: p.offset_accumulate(packed, sums, stream=stream),
+                              p.input_bytes + p.sum_words * 4),
+        "preseed": (lambda: p.preseed(sums, blocks, stream=stream), nb_bytes + p.sum_words * 4),
+        "blocks_to_triangle": (lambda: p.blocks_to_triangle(blocks, tri, stream=stream),
+                               nb_bytes + p.triangle_words * 4),
+        "blocks_to_full": (lambda: p.blocks_to_full(blocks, full, stream=stream),
+                           nb_bytes + full.numel() * 4),
+    }
+    peaks = B.load_peaks() or {}
+    hbm = float(peaks.get("hbm_gbs") or 6650.0)
+    out = {}
+    reps = max(10, min(args.steps, 100))
+    for name, (fn, nbytes) in cases.items():
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize(dev)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = B.max_over_ranks(a.elapsed_time(b) / reps, dist, dev)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "bytes": nbytes, "gbs": gbs, "frac_of_hbm": gbs / hbm}
+    p.check_device()
+    if rank == 0:
+        print(json.dumps({"metric": "HBM GB/s of the helper kernels", "unit": "GB/s",
+                          "config": {"E": E, "F": F, "T": T}, "reps": reps,
+                          "hbm_peak_gbs": hbm,
+                          "peak_source": "measured copy bandwidth (MEASURED_PEAKS.json)"
+                          if peaks.get("hbm_gbs") else "fallback 6650 GB/s",
+                          "kernels": out}))

@@ -5,6 +5,8 @@
 //   * offset_accumulate: offsetAccumulateElements (offset_accumulator.cl:7-49),
 //   * preseed: the four preseed variants (preseed_multifreq*_UT.cl),
 //   * block -> triangle / full-matrix reorganisation (gpu_data_reorg.c:36-124).
+#include <algorithm>
+
 #include "chimex_internal.h"
 
 namespace chx {
@@ -161,34 +163,57 @@ correlate_simt_kernel(const uint8_t *__restrict__ packed, int32_t *__restrict__ 
         }
 }
 
-// offsetAccumulateElements: each thread owns 4 consecutive (f, e) bytes and a
-// sample range; nibbles are summed four lanes at a time in byte-wide SWAR
-// registers (15 * 16 < 256) and flushed to 32-bit sums every 16 samples.
+// offsetAccumulateElements: each thread owns 16 consecutive (f, e) bytes (one
+// 16-byte vector of a sample row) and a sample range; it loads 16 samples'
+// vectors at once (enough bytes in flight to keep HBM busy), sums the nibbles
+// four lanes at a time in byte-wide SWAR registers (15 * 16 < 256) and
+// flushes them to 32-bit sums every 16 samples; the sample ranges meet by
+// atomic add.
 __global__ void __launch_bounds__(256)
 offset_accumulate_kernel(const uint8_t *__restrict__ packed, uint32_t *__restrict__ sums,
-                         int64_t nwords, int T, int tchunk) {
+                         int64_t nvec, int T, int tchunk) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nwords) return;
+    if (i >= nvec) return;
     const int t_begin = blockIdx.y * tchunk;
     const int t_end = min(T, t_begin + tchunk);
-    const uint32_t *p = reinterpret_cast<const uint32_t *>(packed);
-    uint32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint4 *p = reinterpret_cast<const uint4 *>(packed);
+    uint32_t s[32];  // element 4q + j: s[2 (4q + j)] re, s[2 (4q + j) + 1] im
+#pragma unroll
+    for (int k = 0; k < 32; k++) s[k] = 0u;
     for (int t = t_begin; t < t_end; t += 16) {
-        uint32_t lo4 = 0, hi4 = 0;
-        const int n = min(16, t_end - t);
-        for (int k = 0; k < n; k++) {
-            const uint32_t w = __ldg(p + (int64_t)(t + k) * nwords + i);
-            lo4 += w & 0x0F0F0F0Fu;
-            hi4 += (w >> 4) & 0x0F0F0F0Fu;
+        uint32_t lo[4] = {0u, 0u, 0u, 0u}, hi[4] = {0u, 0u, 0u, 0u};
+        const uint4 *row = p + (int64_t)t * nvec + i;
+        auto add = [&](const uint4 w) {
+            lo[0] += w.x & 0x0F0F0F0Fu;
+            hi[0] += (w.x >> 4) & 0x0F0F0F0Fu;
+            lo[1] += w.y & 0x0F0F0F0Fu;
+            hi[1] += (w.y >> 4) & 0x0F0F0F0Fu;
+            lo[2] += w.z & 0x0F0F0F0Fu;
+            hi[2] += (w.z >> 4) & 0x0F0F0F0Fu;
+            lo[3] += w.w & 0x0F0F0F0Fu;
+            hi[3] += (w.w >> 4) & 0x0F0F0F0Fu;
+        };
+        if (t + 16 <= t_end) {  // a full group: 16 independent loads in flight
+            uint4 w[16];
+#pragma unroll
+            for (int k = 0; k < 16; k++) w[k] = __ldg(row + (int64_t)k * nvec);
+#pragma unroll
+            for (int k = 0; k < 16; k++) add(w[k]);
+        } else {
+            for (int k = 0; t + k < t_end; k++) add(__ldg(row + (int64_t)k * nvec));
         }
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            s[2 * j] += (hi4 >> (8 * j)) & 0xFF;
-            s[2 * j + 1] += (lo4 >> (8 * j)) & 0xFF;
+        for (int q = 0; q < 4; q++) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                s[2 * (4 * q + j)] += (hi[q] >> (8 * j)) & 0xFFu;
+                s[2 * (4 * q + j) + 1] += (lo[q] >> (8 * j)) & 0xFFu;
+            }
         }
     }
+    uint32_t *dst = sums + 32 * i;
 #pragma unroll
-    for (int j = 0; j < 8; j++) atomicAdd(sums + 8 * i + j, s[j]);
+    for (int k = 0; k < 32; k++) atomicAdd(dst + k, s[k]);
 }
 
 // preseed: writes (=) the offset correction of every cell of one block.
@@ -246,10 +271,14 @@ blocks_to_triangle_kernel(const int32_t *__restrict__ blocks, int32_t *__restric
     }
 }
 
-// Block layout -> full Hermitian matrix (gpu_data_reorg.c:36-74).
+// Block layout -> full Hermitian matrix (gpu_data_reorg.c:36-74).  The upper
+// triangle is written row by row straight from the block; the mirrored lower
+// triangle (conjugates) goes through a shared-memory transpose so that its
+// rows are written contiguously too.
 __global__ void __launch_bounds__(256)
 blocks_to_full_kernel(const int32_t *__restrict__ blocks, int32_t *__restrict__ full,
                       int E, int nb1, int64_t nb) {
+    __shared__ int2 tile[32][33];
     const int b = blockIdx.x, f = blockIdx.y;
     int by, bx;
     decode_block(b, nb1, by, bx);
@@ -259,12 +288,19 @@ blocks_to_full_kernel(const int32_t *__restrict__ blocks, int32_t *__restrict__ 
     for (int k = 0; k < 4; k++) {
         const int c = threadIdx.x + 256 * k, yl = c >> 5, xl = c & 31;
         const int64_t y = by * 32 + yl, x = bx * 32 + xl;
-        if (x < y) continue;
         const int2 v = *reinterpret_cast<const int2 *>(blk + 2 * c);
-        *reinterpret_cast<int2 *>(m + (y * E + x) * 2) = v;
-        if (x > y)
-            *reinterpret_cast<int2 *>(m + (x * E + y) * 2) =
-                make_int2(v.x, (int)(0u - (uint32_t)v.y));
+        tile[yl][xl] = v;
+        if (x >= y) *reinterpret_cast<int2 *>(m + (y * E + x) * 2) = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int c = threadIdx.x + 256 * k, xl = c >> 5, yl = c & 31;
+        const int64_t y = by * 32 + yl, x = bx * 32 + xl;
+        if (x > y) {
+            const int2 v = tile[yl][xl];
+            *reinterpret_cast<int2 *>(m + (x * E + y) * 2) = make_int2(v.x, (int)(0u - (uint32_t)v.y));
+        }
     }
 }
 
@@ -291,10 +327,16 @@ cudaError_t launch_correlate_simt(const uint8_t *packed, int32_t *blocks, int E,
 
 cudaError_t launch_offset_accumulate(const uint8_t *packed, uint32_t *sums, int E, int F,
                                      int T, cudaStream_t st) {
-    const int64_t nwords = (int64_t)F * E / 4;
-    const int tchunk = 512;
-    dim3 grid((unsigned)((nwords + 255) / 256), (unsigned)((T + tchunk - 1) / tchunk));
-    offset_accumulate_kernel<<<grid, 256, 0, st>>>(packed, sums, nwords, T, tchunk);
+    const int64_t nvec = (int64_t)F * E / 16;  // E % 32 == 0
+    // About 64k threads in all (each with 16 x 16 bytes in flight per group),
+    // sample ranges of a multiple of 16 samples, at most 65535 of them; long
+    // ranges keep the atomic flushes few.
+    int64_t chunks = std::max<int64_t>(1, 65536 / std::max<int64_t>(1, nvec));
+    chunks = std::min<int64_t>(chunks, (T + 15) / 16);
+    int tchunk = (int)(((T + chunks - 1) / chunks + 15) / 16 * 16);
+    while ((T + tchunk - 1) / tchunk > 65535) tchunk += 16;
+    dim3 grid((unsigned)((nvec + 255) / 256), (unsigned)((T + tchunk - 1) / tchunk));
+    offset_accumulate_kernel<<<grid, 256, 0, st>>>(packed, sums, nvec, T, tchunk);
     return cudaGetLastError();
 }
 
