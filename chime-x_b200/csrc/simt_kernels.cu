@@ -234,21 +234,30 @@ preseed_kernel(const uint32_t *__restrict__ sums, int32_t *__restrict__ blocks, 
     }
     __syncthreads();
     int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
+    // Two neighbouring cells (xl, xl + 1) per 16-byte store.
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int c = tid + 256 * k, yl = c >> 5, xl = c & 31;
-        const uint32_t xr = sx[2 * xl], xi = sx[2 * xl + 1];
+    for (int k = 0; k < 2; k++) {
+        const int c2 = tid + 256 * k, yl = c2 >> 4, xl0 = (c2 & 15) * 2;
         const uint32_t yr = sy[2 * yl], yi = sy[2 * yl + 1];
-        uint32_t re, imv;
-        if (!packed_variant) {
-            re = t128 - 8u * (xr + xi + yr + yi);
-            imv = ut ? 8u * ((xi - xr) + (yr - yi)) : 8u * ((xr - xi) + (yi - yr));
-        } else {
-            re = t128 - 8u * xr + 7u * xi - 8u * (yr + yi);
-            imv = ut ? 8u * xi + 7u * xr + 8u * (yr - yi)
-                     : 0u - 8u * xi - 7u * xr - 8u * (yr - yi);
+        uint32_t v[4];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int xl = xl0 + h;
+            const uint32_t xr = sx[2 * xl], xi = sx[2 * xl + 1];
+            uint32_t re, imv;
+            if (!packed_variant) {
+                re = t128 - 8u * (xr + xi + yr + yi);
+                imv = ut ? 8u * ((xi - xr) + (yr - yi)) : 8u * ((xr - xi) + (yi - yr));
+            } else {
+                re = t128 - 8u * xr + 7u * xi - 8u * (yr + yi);
+                imv = ut ? 8u * xi + 7u * xr + 8u * (yr - yi)
+                         : 0u - 8u * xi - 7u * xr - 8u * (yr - yi);
+            }
+            v[2 * h] = re;
+            v[2 * h + 1] = imv;
         }
-        *reinterpret_cast<int2 *>(blk + c * 2) = make_int2((int)re, (int)imv);
+        *reinterpret_cast<int4 *>(blk + (yl * 32 + xl0) * 2) =
+            make_int4((int)v[0], (int)v[1], (int)v[2], (int)v[3]);
     }
 }
 
