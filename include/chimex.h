@@ -192,6 +192,8 @@ typedef struct chx_channel_desc {
     int32_t *d_blocks;     /* num_integrations block buffers of NB_c*2048 */
 } chx_channel_desc;
 
+/* A batch is thread-compatible like a plan: one thread at a time per batch.
+ * Its channels' buffers stay owned by the caller and must outlive it. */
 typedef struct chx_batch chx_batch;
 
 /* Builds the tile queue for n channels.  The descriptors are copied.  The
@@ -231,6 +233,8 @@ int chx_autotune(int num_elements, int num_timesamples, const uint8_t *d_scratch
  * stream (the integration accumulates in tensor memory and is written to its
  * dump buffer once).
  * ------------------------------------------------------------------- */
+/* A stream is driven by one host thread at a time (admit, submit, stats);
+ * its completion thread only publishes finished dumps. */
 typedef struct chx_stream chx_stream;
 
 typedef struct chx_stream_stats {
