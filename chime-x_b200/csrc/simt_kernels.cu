@@ -219,22 +219,12 @@ offset_accumulate_kernel(const uint8_t *__restrict__ packed, uint32_t *__restric
 // preseed: writes (=) the offset correction of every cell of one block.
 // Formulas: preseed_multifreq_UT.cl:54-70 / preseed_multifreq.cl:54-70
 // (conference) and preseed_multifreq_highly_packed_correlator_method{_UT,}.cl
-// :54-70 (packed); x is the column element, y the row element.
-__global__ void __launch_bounds__(256)
-preseed_kernel(const uint32_t *__restrict__ sums, int32_t *__restrict__ blocks, int E,
-               int nb1, int64_t nb, uint32_t t128, int packed_variant, int ut) {
-    __shared__ uint32_t sx[64], sy[64];
-    const int b = blockIdx.x, f = blockIdx.y;
-    int by, bx;
-    decode_block(b, nb1, by, bx);
-    const int tid = threadIdx.x;
-    if (tid < 64) {
-        sx[tid] = sums[((int64_t)f * E + bx * 32) * 2 + tid];
-        sy[tid] = sums[((int64_t)f * E + by * 32) * 2 + tid];
-    }
-    __syncthreads();
-    int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
-    // Two neighbouring cells (xl, xl + 1) per 16-byte store.
+// :54-70 (packed); x is the column element, y the row element.  sx / sy hold
+// the (re, im) sums of the block's 32 columns / rows; 256 threads write two
+// neighbouring cells (xl, xl + 1) per 16-byte store.
+__device__ __forceinline__ void preseed_block(const uint32_t *sx, const uint32_t *sy,
+                                              int32_t *blk, uint32_t t128,
+                                              int packed_variant, int ut, int tid) {
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         const int c2 = tid + 256 * k, yl = c2 >> 4, xl0 = (c2 & 15) * 2;
@@ -259,6 +249,25 @@ preseed_kernel(const uint32_t *__restrict__ sums, int32_t *__restrict__ blocks, 
         *reinterpret_cast<int4 *>(blk + (yl * 32 + xl0) * 2) =
             make_int4((int)v[0], (int)v[1], (int)v[2], (int)v[3]);
     }
+}
+
+// One CTA per block: 16.6k CTAs at E = 2048, F = 8 keep enough stores in
+// flight (a CTA per run of blocks, with the channel's sums in shared memory,
+// measured 1.8x slower).
+__global__ void __launch_bounds__(256)
+preseed_kernel(const uint32_t *__restrict__ sums, int32_t *__restrict__ blocks, int E,
+               int nb1, int64_t nb, uint32_t t128, int packed_variant, int ut) {
+    __shared__ uint32_t sx[64], sy[64];
+    const int b = blockIdx.x, f = blockIdx.y;
+    int by, bx;
+    decode_block(b, nb1, by, bx);
+    const int tid = threadIdx.x;
+    if (tid < 64) {
+        sx[tid] = sums[((int64_t)f * E + bx * 32) * 2 + tid];
+        sy[tid] = sums[((int64_t)f * E + by * 32) * 2 + tid];
+    }
+    __syncthreads();
+    preseed_block(sx, sy, blocks + ((int64_t)f * nb + b) * 2048, t128, packed_variant, ut, tid);
 }
 
 // Block layout -> packed triangle (gpu_data_reorg.c:76-124).
@@ -351,9 +360,10 @@ cudaError_t launch_offset_accumulate(const uint8_t *packed, uint32_t *sums, int 
 
 cudaError_t launch_preseed(const uint32_t *sums, int32_t *blocks, int E, int F, int T,
                            int packed_variant, int ut, cudaStream_t st) {
-    dim3 grid((unsigned)num_blocks_of(E), (unsigned)F);
-    preseed_kernel<<<grid, 256, 0, st>>>(sums, blocks, E, E / 32, num_blocks_of(E),
-                                         (uint32_t)T * 128u, packed_variant, ut);
+    const int64_t nb = num_blocks_of(E);
+    dim3 grid((unsigned)nb, (unsigned)F);
+    preseed_kernel<<<grid, 256, 0, st>>>(sums, blocks, E, E / 32, nb, (uint32_t)T * 128u,
+                                         packed_variant, ut);
     return cudaGetLastError();
 }
 
