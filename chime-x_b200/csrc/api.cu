@@ -70,13 +70,8 @@ cudaError_t build_tc_tables(chx_plan *p) {
         if (!split) split = tuned_split;
     }
     if (!tile) tile = tc_default_tile(p->E);
-    for (int f = 0; f < p->F; f++) {
-        if (tile == kTile2Sm)
-            tc_append_pair_units(units, f, p->E, 0, p->T, split, 0);
-        else
-            tc_append_units(units, f, p->E, 0, p->T, split, 0);
-    }
-    const int slots = tile == kTile2Sm ? p->sm_count / 2 : p->sm_count;
+    for (int f = 0; f < p->F; f++) tc_append_tile_units(tile, units, f, p->E, 0, p->T, split, 0);
+    const int slots = tc_tile_slots(tile, p->sm_count);
     const int grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, slots));
     std::vector<int> offsets;
     tc_schedule(units, grid, offsets);
@@ -133,10 +128,7 @@ int run_tc(chx_plan *p, const uint8_t *d_packed, int32_t *d_blocks, int map, int
     L.accumulate = accumulate;
     L.err = p->d_err;
     L.grid = p->grid;
-    if (p->tile_built == kTile2Sm)
-        CHX_CUDA(tc_pair_launch(L, &tmap, &omap, st));
-    else
-        CHX_CUDA(tc_launch(L, &tmap, &omap, st));
+    CHX_CUDA(tc_tile_launch(p->tile_built, L, &tmap, &omap, st));
     return CHX_OK;
 }
 
@@ -230,8 +222,9 @@ int chx_plan_set_option(chx_plan *p, int option, int64_t value) {
         return CHX_OK;
     }
     case CHX_OPT_TILE: {
-        if (value < 0 || value > kTile2Sm)
-            return fail(CHX_E_INVALID, "tile variant %lld (0 auto, 1 one SM, 2 SM pair)",
+        if (value < 0 || value > kTileMax)
+            return fail(CHX_E_INVALID,
+                        "tile variant %lld (0 auto, 1 one SM, 2 SM pair)",
                         (long long)value);
         p->tile = (int)value;
         DeviceGuard g(p->device);

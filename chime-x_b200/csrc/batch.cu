@@ -113,10 +113,7 @@ int record_batch(chx_batch *b, cudaStream_t st, int accumulate) {
     L.accumulate = accumulate;
     L.err = b->d_err;
     L.grid = b->grid;
-    if (b->tile == kTile2Sm)
-        CHX_CUDA(tc_pair_launch(L, nullptr, nullptr, st));
-    else
-        CHX_CUDA(tc_launch(L, nullptr, nullptr, st));
+    CHX_CUDA(tc_tile_launch(b->tile, L, nullptr, nullptr, st));
     return CHX_OK;
 }
 
@@ -217,17 +214,15 @@ int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int 
         for (int i = 0; i < d.num_integrations; i++) {
             const size_t before = units.size();
             const int t0 = i * d.num_timesamples, t1 = t0 + d.num_timesamples;
-            if (b->tile == kTile2Sm)
-                tc_append_pair_units(units, c, d.num_elements, t0, t1, split, (long long)i * nb * 2048);
-            else
-                tc_append_units(units, c, d.num_elements, t0, t1, split, (long long)i * nb * 2048);
+            tc_append_tile_units(b->tile, units, c, d.num_elements, t0, t1, split,
+                                 (long long)i * nb * 2048);
             bool any_split = false;
             for (size_t k = before; k < units.size(); k++) any_split |= units[k].split != 0;
             if (any_split)
                 b->zero_regions.push_back({d.d_blocks + (size_t)i * nb * 2048, (size_t)nb * 2048 * 4});
         }
     }
-    const int slots = b->tile == kTile2Sm ? sm_count / 2 : sm_count;
+    const int slots = tc_tile_slots(b->tile, sm_count);
     b->grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, slots));
     std::vector<int> offsets;
     tc_schedule(units, b->grid, offsets);

@@ -184,7 +184,15 @@ cudaError_t tc_pair_launch(const TcLaunch &L, const CUtensorMap *param_map,
 // Tensor-core tile variants (CHX_OPT_TILE).
 constexpr int kTile1Sm = 1;  // 128 x 256 elements per CTA
 constexpr int kTile2Sm = 2;  // 256 x 256 elements per CTA pair
+constexpr int kTileMax = kTile2Sm;
 int tc_default_tile(int E);
+// Dispatch by tile variant: units of one channel's sample range, persistent
+// CTAs (or clusters) for `sm_count` SMs, and the launch.
+void tc_append_tile_units(int tile, std::vector<Unit> &out, int chan, int E, int t_begin,
+                          int t_end, int tsplit, long long out_off);
+int tc_tile_slots(int tile, int sm_count);
+cudaError_t tc_tile_launch(int tile, const TcLaunch &L, const CUtensorMap *param_map,
+                           const CUtensorMap *param_omap, cudaStream_t st);
 // The autotuner's cached choice for (device, E, T) (batch.cu): true and the
 // tile variant and split count when an entry with the same E and a T within a
 // factor 2 exists.

@@ -493,6 +493,24 @@ int tc_default_tile(int E) {
     return (nt % 2 == 0) ? kTile2Sm : kTile1Sm;
 }
 
+void tc_append_tile_units(int tile, std::vector<Unit> &out, int chan, int E, int t_begin,
+                          int t_end, int tsplit, long long out_off) {
+    if (tile == kTile2Sm)
+        tc_append_pair_units(out, chan, E, t_begin, t_end, tsplit, out_off);
+    else
+        tc_append_units(out, chan, E, t_begin, t_end, tsplit, out_off);
+}
+
+int tc_tile_slots(int tile, int sm_count) {
+    return tile == kTile2Sm ? sm_count / 2 : sm_count;
+}
+
+cudaError_t tc_tile_launch(int tile, const TcLaunch &L, const CUtensorMap *param_map,
+                           const CUtensorMap *param_omap, cudaStream_t st) {
+    if (tile == kTile2Sm) return tc_pair_launch(L, param_map, param_omap, st);
+    return tc_launch(L, param_map, param_omap, st);
+}
+
 bool tc_supported(int E, int T) { return E >= 32 && E % 32 == 0 && E <= 65536 && T >= 1; }
 
 void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t_end, int tsplit,
