@@ -50,6 +50,17 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+def sum_over_ranks(value, dist, device):
+    """The sum of `value` over all ranks; `value` itself when there is no
+    process group."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def env_rank():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
             int(os.environ.get("WORLD_SIZE", 1)))

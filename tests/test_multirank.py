@@ -1,7 +1,7 @@
 """Multi-process logic of bench.py on CPU (gloo, world size 2): channels are
 independent, so ranks share nothing on the data path; the only cross-rank
-steps are the barrier around the timed region and the max-over-ranks of the
-device times, and only rank 0 prints."""
+steps are the barrier around the timed region, the max-over-ranks of the
+device times and the sum of per-rank counts, and only rank 0 prints."""
 import json
 import os
 import socket
@@ -36,8 +36,9 @@ def _rank_main(rank, world, port, out_dir):
         local_ms = 10.0 + 5.0 * rank  # rank 1 is the slow one
         dist.barrier()
         job_ms = bench.max_over_ranks(local_ms, dist, "cpu")
+        job_channels = bench.sum_over_ranks(100 + rank, dist, "cpu")  # per-rank counts add up
         with open(os.path.join(out_dir, "rank%d.json" % rank), "w") as fh:
-            json.dump({"env": [r, lr, w], "job_ms": job_ms}, fh)
+            json.dump({"env": [r, lr, w], "job_ms": job_ms, "job_channels": job_channels}, fh)
     finally:
         dist.destroy_process_group()
 
@@ -51,12 +52,14 @@ def test_max_over_ranks_with_gloo(tmp_path):
         rec = json.load(open(tmp_path / ("rank%d.json" % rank)))
         assert rec["env"] == [rank, rank, 2]
         assert rec["job_ms"] == 15.0
+        assert rec["job_channels"] == 201.0
 
 
 def test_max_over_ranks_without_group():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+    assert bench.sum_over_ranks(7.0, None, "cpu") == 7.0
 
 
 def test_reference_arm_under_torchrun_prints_once():
