@@ -163,57 +163,74 @@ correlate_simt_kernel(const uint8_t *__restrict__ packed, int32_t *__restrict__ 
         }
 }
 
-// offsetAccumulateElements: each thread owns 16 consecutive (f, e) bytes (one
-// 16-byte vector of a sample row) and a sample range; it loads 16 samples'
-// vectors at once (enough bytes in flight to keep HBM busy), sums the nibbles
-// four lanes at a time in byte-wide SWAR registers (15 * 16 < 256) and
-// flushes them to 32-bit sums every 16 samples; the sample ranges meet by
-// atomic add.
-__global__ void __launch_bounds__(256)
+// offsetAccumulateElements (offset_accumulator.cl:18-47).  A CTA owns 32
+// consecutive 16-byte vectors of a sample row (16 (f, e) bytes each) and a
+// sample range; warp w streams the range's 16-sample groups w, w + 8, ...
+// (each lane one vector: coalesced 512-byte rows), loading a group's 16
+// vectors at once so that enough bytes are in flight to keep HBM busy.  The
+// nibbles are summed four lanes at a time in byte-wide SWAR registers
+// (15 * 16 < 256) and flushed to 32-bit sums after every group; the 8 warps'
+// sums meet in shared memory, and the CTAs' in one atomic add per word.
+constexpr int kOaWarps = 8;
+
+__global__ void __launch_bounds__(kOaWarps * 32)
 offset_accumulate_kernel(const uint8_t *__restrict__ packed, uint32_t *__restrict__ sums,
                          int64_t nvec, int T, int tchunk) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nvec) return;
+    __shared__ uint32_t part[kOaWarps][32][32];  // [warp][word][lane]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t i = (int64_t)blockIdx.x * 32 + lane;
     const int t_begin = blockIdx.y * tchunk;
     const int t_end = min(T, t_begin + tchunk);
     const uint4 *p = reinterpret_cast<const uint4 *>(packed);
     uint32_t s[32];  // element 4q + j: s[2 (4q + j)] re, s[2 (4q + j) + 1] im
 #pragma unroll
     for (int k = 0; k < 32; k++) s[k] = 0u;
-    for (int t = t_begin; t < t_end; t += 16) {
-        uint32_t lo[4] = {0u, 0u, 0u, 0u}, hi[4] = {0u, 0u, 0u, 0u};
-        const uint4 *row = p + (int64_t)t * nvec + i;
-        auto add = [&](const uint4 w) {
-            lo[0] += w.x & 0x0F0F0F0Fu;
-            hi[0] += (w.x >> 4) & 0x0F0F0F0Fu;
-            lo[1] += w.y & 0x0F0F0F0Fu;
-            hi[1] += (w.y >> 4) & 0x0F0F0F0Fu;
-            lo[2] += w.z & 0x0F0F0F0Fu;
-            hi[2] += (w.z >> 4) & 0x0F0F0F0Fu;
-            lo[3] += w.w & 0x0F0F0F0Fu;
-            hi[3] += (w.w >> 4) & 0x0F0F0F0Fu;
-        };
-        if (t + 16 <= t_end) {  // a full group: 16 independent loads in flight
-            uint4 w[16];
+    if (i < nvec) {
+        for (int t = t_begin + 16 * w; t < t_end; t += 16 * kOaWarps) {
+            uint32_t lo[4] = {0u, 0u, 0u, 0u}, hi[4] = {0u, 0u, 0u, 0u};
+            const uint4 *row = p + (int64_t)t * nvec + i;
+            auto add = [&](const uint4 v) {
+                lo[0] += v.x & 0x0F0F0F0Fu;
+                hi[0] += (v.x >> 4) & 0x0F0F0F0Fu;
+                lo[1] += v.y & 0x0F0F0F0Fu;
+                hi[1] += (v.y >> 4) & 0x0F0F0F0Fu;
+                lo[2] += v.z & 0x0F0F0F0Fu;
+                hi[2] += (v.z >> 4) & 0x0F0F0F0Fu;
+                lo[3] += v.w & 0x0F0F0F0Fu;
+                hi[3] += (v.w >> 4) & 0x0F0F0F0Fu;
+            };
+            if (t + 16 <= t_end) {  // a full group: 16 independent loads in flight
+                uint4 v[16];
 #pragma unroll
-            for (int k = 0; k < 16; k++) w[k] = __ldg(row + (int64_t)k * nvec);
+                for (int k = 0; k < 16; k++) v[k] = __ldg(row + (int64_t)k * nvec);
 #pragma unroll
-            for (int k = 0; k < 16; k++) add(w[k]);
-        } else {
-            for (int k = 0; t + k < t_end; k++) add(__ldg(row + (int64_t)k * nvec));
-        }
+                for (int k = 0; k < 16; k++) add(v[k]);
+            } else {
+                for (int k = 0; t + k < t_end; k++) add(__ldg(row + (int64_t)k * nvec));
+            }
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < 4; q++) {
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                s[2 * (4 * q + j)] += (hi[q] >> (8 * j)) & 0xFFu;
-                s[2 * (4 * q + j) + 1] += (lo[q] >> (8 * j)) & 0xFFu;
+                for (int j = 0; j < 4; j++) {
+                    s[2 * (4 * q + j)] += (hi[q] >> (8 * j)) & 0xFFu;
+                    s[2 * (4 * q + j) + 1] += (lo[q] >> (8 * j)) & 0xFFu;
+                }
             }
         }
     }
-    uint32_t *dst = sums + 32 * i;
 #pragma unroll
-    for (int k = 0; k < 32; k++) atomicAdd(dst + k, s[k]);
+    for (int k = 0; k < 32; k++) part[w][k][lane] = s[k];
+    __syncthreads();
+    // Thread r handles (word, lane) pairs r, r + 256, ...: sum over the warps.
+#pragma unroll
+    for (int r = threadIdx.x; r < 32 * 32; r += kOaWarps * 32) {
+        const int k = r >> 5, l = r & 31;
+        const int64_t iv = (int64_t)blockIdx.x * 32 + l;
+        uint32_t acc = 0u;
+#pragma unroll
+        for (int ww = 0; ww < kOaWarps; ww++) acc += part[ww][k][l];
+        if (iv < nvec && acc != 0u) atomicAdd(sums + 32 * iv + k, acc);
+    }
 }
 
 // preseed: writes (=) the offset correction of every cell of one block.
@@ -346,15 +363,20 @@ cudaError_t launch_correlate_simt(const uint8_t *packed, int32_t *blocks, int E,
 cudaError_t launch_offset_accumulate(const uint8_t *packed, uint32_t *sums, int E, int F,
                                      int T, cudaStream_t st) {
     const int64_t nvec = (int64_t)F * E / 16;  // E % 32 == 0
-    // About 64k threads in all (each with 16 x 16 bytes in flight per group),
-    // sample ranges of a multiple of 16 samples, at most 65535 of them; long
-    // ranges keep the atomic flushes few.
-    int64_t chunks = std::max<int64_t>(1, 65536 / std::max<int64_t>(1, nvec));
-    chunks = std::min<int64_t>(chunks, (T + 15) / 16);
-    int tchunk = (int)(((T + chunks - 1) / chunks + 15) / 16 * 16);
-    while ((T + tchunk - 1) / tchunk > 65535) tchunk += 16;
-    dim3 grid((unsigned)((nvec + 255) / 256), (unsigned)((T + tchunk - 1) / tchunk));
-    offset_accumulate_kernel<<<grid, 256, 0, st>>>(packed, sums, nvec, T, tchunk);
+    const int64_t vblocks = (nvec + 31) / 32;
+    // One wave: three CTAs per SM fit (66 registers, 32 KiB shared memory),
+    // and a single wave beat two to four on B200 (4.66 vs 3.92 TB/s at E=2048,
+    // F=8, T=16384).  Sample ranges are a multiple of 8 warps x 16 samples,
+    // at most 65535 of them.
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int64_t chunks = std::max<int64_t>(1, (int64_t)3 * sms / std::max<int64_t>(1, vblocks));
+    chunks = std::min<int64_t>(chunks, (T + 127) / 128);
+    int tchunk = (int)(((T + chunks - 1) / chunks + 127) / 128 * 128);
+    while ((T + tchunk - 1) / tchunk > 65535) tchunk += 128;
+    dim3 grid((unsigned)vblocks, (unsigned)((T + tchunk - 1) / tchunk));
+    offset_accumulate_kernel<<<grid, kOaWarps * 32, 0, st>>>(packed, sums, nvec, T, tchunk);
     return cudaGetLastError();
 }
 
