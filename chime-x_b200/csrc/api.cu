@@ -70,6 +70,7 @@ cudaError_t build_tc_tables(chx_plan *p) {
         if (!split) split = tuned_split;
     }
     if (!tile) tile = tc_default_tile(p->E);
+    if (!split) split = tc_auto_split(tile, p->E, p->F, p->T, p->sm_count);
     for (int f = 0; f < p->F; f++) tc_append_tile_units(tile, units, f, p->E, 0, p->T, split, 0);
     const int slots = tc_tile_slots(tile, p->sm_count);
     const int grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, slots));

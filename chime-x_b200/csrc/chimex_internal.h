@@ -48,7 +48,7 @@ struct chx_plan {
     int nunits;
     int grid;       // persistent CTAs (or CTA pairs) of a tensor-core launch
     int tile_built; // tile variant the tables were built for
-    bool has_split_units;  // some output cells receive several units (atomic)
+    bool has_split_units;  // some output cells receive several units (TMA reduce-add)
 };
 
 namespace chx {
@@ -131,7 +131,7 @@ struct Unit {
     int tyx;
     int t0, t1;
     long long out_off;  // int32 words added to the channel's block buffer
-    int split;          // 1: other units add to the same cells (atomic add)
+    int split;          // 1: other units add to the same cells (TMA reduce-add)
     int cost;           // samples x x-tiles, for scheduling
 };
 static_assert(sizeof(Unit) == 32, "Unit layout");
@@ -159,6 +159,12 @@ void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t
 // Assigns units to `grid` persistent CTAs (longest first, to the least
 // loaded CTA) and reorders them CTA by CTA; offsets gets grid + 1 entries.
 void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets);
+// Makespan, in unit-cost units, of that assignment when every unit also pays
+// `handoff_stages` of its stages for the accumulator hand-off.
+long long tc_estimate_makespan(const std::vector<Unit> &u, int grid, int handoff_stages);
+// Number of sample-range splits (1-8) with the shortest estimated makespan
+// for F channels of E elements and T samples on the tile variant.
+int tc_auto_split(int tile, int E, int F, int T, int sm_count);
 // Encodes the TMA map of packed samples: dims {E, channels, samples}.
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
                   int64_t chan_stride, int64_t sample_stride);

@@ -45,6 +45,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
+#include <queue>
 
 namespace chx {
 
@@ -361,7 +363,11 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
             const int q = warp & 3, h = warp >> 2;  // lane quarter, column group
             const int nb1 = cd->nb1;
             const int by = ty * 4 + q;
-            const int mode = U.split ? 2 : (P.accumulate ? 1 : 0);
+            // Split units (other units cover the same cells' other sample ranges)
+            // add like accumulate mode: every element of a TMA reduce-add is an
+            // individual relaxed reduction at gpu scope, so concurrent units meet
+            // exactly in the zeroed (or accumulating) output.
+            const bool add = U.split || P.accumulate;
             const CUtensorMap *omap = P.use_param_map ? &pomap : &cd->omap;
             const int row0 = cd->orow + (int)(U.out_off >> 6);
             uint32_t nchunk = 0;
@@ -377,10 +383,8 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                     // Stage the 32 x 32-word tile (rows = lanes) in two
                     // 8-column parts, then hand it to TMA.
                     const uint32_t tile = stage + (nchunk % (uint32_t)kEpiTiles) * 4096u;
-                    if (mode != 2) {
-                        if (lane == 0) bulk_wait_read<kEpiTiles - 1>();
-                        __syncwarp();
-                    }
+                    if (lane == 0) bulk_wait_read<kEpiTiles - 1>();
+                    __syncwarp();
 #pragma unroll
                     for (int part = 0; part < 2; part++) {
                         uint32_t re[8], im[8];
@@ -393,27 +397,16 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                             im[k] = (uint32_t)((int32_t)im[k] >> 4);
                             if (!P.ut) im[k] = 0u - im[k];
                         }
-                        if (mode == 2) {  // split units: other units add to these cells
-                            int32_t *d = reinterpret_cast<int32_t *>(P.out_base + cd->out) +
-                                         U.out_off + (b * 32 + lane) * 64 + 32 * half + 16 * part;
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                atomicAdd(d + 2 * k, (int)re[k]);
-                                atomicAdd(d + 2 * k + 1, (int)im[k]);
-                            }
-                        } else {
-                            stage_row_half(tile, lane, part, re, im);
-                        }
+                        stage_row_half(tile, lane, part, re, im);
                     }
-                    if (mode == 2) continue;
                     fence_proxy_async();
                     __syncwarp();
                     if (lane == 0) {
                         const int y = row0 + (int)b * 32;
-                        if (mode == 0)
-                            tma_store_2d(omap, tile, 32 * half, y);
-                        else
+                        if (add)
                             tma_add_2d(omap, tile, 32 * half, y);
+                        else
+                            tma_store_2d(omap, tile, 32 * half, y);
                         bulk_commit();
                     }
                     nchunk++;
@@ -570,6 +563,60 @@ void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets) {
     std::vector<Unit> out(u.size());
     for (size_t i = 0; i < u.size(); i++) out[fill[owner[i]]++] = u[i];
     u.swap(out);
+}
+
+long long tc_estimate_makespan(const std::vector<Unit> &u, int grid, int handoff_stages) {
+    if (grid < 1) grid = 1;
+    std::vector<long long> cost(u.size());
+    for (size_t i = 0; i < u.size(); i++) {
+        const long long st = std::max(1, (u[i].t1 - u[i].t0 + kStageSamples - 1) / kStageSamples);
+        cost[i] = u[i].cost + (long long)handoff_stages * u[i].cost / st;
+    }
+    std::sort(cost.begin(), cost.end(), std::greater<long long>());
+    std::priority_queue<long long, std::vector<long long>, std::greater<long long>> load;
+    for (int b = 0; b < grid; b++) load.push(0);
+    long long span = 0;
+    for (long long c : cost) {
+        const long long l = load.top() + c;
+        load.pop();
+        load.push(l);
+        span = std::max(span, l);
+    }
+    return span;
+}
+
+int tc_auto_split(int tile, int E, int F, int T, int sm_count) {
+    // A unit's accumulator hand-off costs about as much as 11 of its stages in
+    // the SM-pair kernel (measured on B200: ~9,400 cycles against ~850 per
+    // stage) and about 16 in the one-SM kernel, whose unpack warps run the
+    // epilogue themselves.  Splitting a channel's samples therefore pays only
+    // while it fills idle SMs.  With these overheads the estimate came within
+    // 2 % of the best measured split of every shape tried (E = 256-2048,
+    // F = 1-16, T = 16384; e.g. E = 1024, F = 2: 7 splits, 1551 vs 598 TOPS
+    // unsplit; E = 2048, F = 8: no split).  A split must win by 3 % to pay for
+    // zeroing the output and for the reduce-adds.
+    const int handoff_stages = tile == kTile2Sm ? 11 : 16;
+    const int grid_slots = tc_tile_slots(tile, sm_count);
+    long long best = -1;
+    int best_k = 1, last_chunks = 0;
+    for (int k = 1; k <= 8; k++) {
+        std::vector<Unit> units;
+        for (int f = 0; f < F; f++) tc_append_tile_units(tile, units, f, E, 0, T, k, 0);
+        if (units.empty()) return 1;
+        // Ranges are rounded to whole stages: skip counts that give the same cut.
+        const int chunks = (int)std::count_if(units.begin(), units.end(), [&](const Unit &x) {
+            return x.chan == 0 && x.tyx == units[0].tyx;
+        });
+        if (chunks == last_chunks) continue;
+        last_chunks = chunks;
+        const int grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, grid_slots));
+        const long long span = tc_estimate_makespan(units, grid, handoff_stages);
+        if (best < 0 || (k == 1 ? span < best : span * 100 < best * 97)) {
+            best = span;
+            best_k = k;
+        }
+    }
+    return best_k;
 }
 
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,

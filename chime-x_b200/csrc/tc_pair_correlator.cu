@@ -362,7 +362,11 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
             const int tx2 = (U.tyx >> 10) & 1023;
             const int nb1 = cd->nb1;
             const int by = ty * 4 + q;
-            const int mode = U.split ? 2 : (P.accumulate ? 1 : 0);
+            // Split units (other units cover the same cells' other sample ranges)
+            // add like accumulate mode: every element of a TMA reduce-add is an
+            // individual relaxed reduction at gpu scope, so concurrent units meet
+            // exactly in the zeroed (or accumulating) output.
+            const bool add = U.split || P.accumulate;
             const CUtensorMap *omap = P.use_param_map ? &pomap : &cd->omap;
             const int row0 = cd->orow + (int)(U.out_off >> 6);
             if (!mbar_wait(bar(kBarAccFull), acc_phase, abort_flag)) {
@@ -382,10 +386,8 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                     // Stage the 32 x 32-word tile (rows = lanes) in two
                     // 8-column parts, then hand it to TMA.
                     const uint32_t tile = stage + (nchunk % (uint32_t)kEpiTiles) * 4096u;
-                    if (mode != 2) {
-                        if (lane == 0) bulk_wait_read<kEpiTiles - 1>();
-                        __syncwarp();
-                    }
+                    if (lane == 0) bulk_wait_read<kEpiTiles - 1>();
+                    __syncwarp();
 #pragma unroll
                     for (int part = 0; part < 2; part++) {
                         uint32_t re[8], im[8];
@@ -398,27 +400,16 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                             im[k] = (uint32_t)((int32_t)im[k] >> 4);
                             if (!P.ut) im[k] = 0u - im[k];
                         }
-                        if (mode == 2) {  // split units: other units add to these cells
-                            int32_t *d = reinterpret_cast<int32_t *>(P.out_base + cd->out) +
-                                         U.out_off + (b * 32 + lane) * 64 + 32 * half + 16 * part;
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                atomicAdd(d + 2 * k, (int)re[k]);
-                                atomicAdd(d + 2 * k + 1, (int)im[k]);
-                            }
-                        } else {
-                            stage_row_half(tile, lane, part, re, im);
-                        }
+                        stage_row_half(tile, lane, part, re, im);
                     }
-                    if (mode == 2) continue;
                     fence_proxy_async();
                     __syncwarp();
                     if (lane == 0) {
                         const int y = row0 + (int)b * 32;
-                        if (mode == 0)
-                            tma_store_2d(omap, tile, 32 * half, y);
-                        else
+                        if (add)
                             tma_add_2d(omap, tile, 32 * half, y);
+                        else
+                            tma_store_2d(omap, tile, 32 * half, y);
                         bulk_commit();
                     }
                     nchunk++;

@@ -61,7 +61,10 @@ extern "C" {
 
 /* Plan options. */
 #define CHX_OPT_ALGO 1      /* one of CHX_ALGO_* */
-#define CHX_OPT_TSPLIT 2    /* number of sample-range splits (0 = auto) */
+#define CHX_OPT_TSPLIT 2    /* number of sample-range splits: 0 auto (the
+                               autotuned value, else the split with the
+                               shortest estimated makespan, so that few
+                               channels still fill the GPU), n >= 1 fixed */
 #define CHX_OPT_TILE 3      /* tensor-core tile variant: 0 auto (SM pair when
                                ceil(E/128) is even, else one SM), 1 one SM
                                (128 x 256 elements), 2 SM pair (256 x 256) */

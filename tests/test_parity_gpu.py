@@ -117,6 +117,27 @@ def test_sample_splits_and_accumulate(chimex, algo, tsplit):
     np.testing.assert_array_equal(out.cpu().numpy(), (ref.astype(np.int64) * 2).astype(np.int32))
 
 
+@pytest.mark.parametrize("algo", ["tc", "tc2"])
+@pytest.mark.parametrize("tsplit", [0, 2, 5, 16])
+def test_split_units_meet_by_reduce_add(chimex, algo, tsplit):
+    """The sample ranges of one tile pair run as separate units on different
+    CTAs at the same time and add into the zeroed (or accumulating) output with
+    TMA reduce-adds; repeated runs must equal the unsplit dp4a result exactly.
+    tsplit 0 takes the automatic choice (this small shape is split)."""
+    E, F, T = 512, 2, 4096
+    packed = orc.generate(T, F, E, 4, 91, no_repeat=1)
+    d = to_dev(packed)
+    want = make_plan(chimex, E, F, T, algo="simt").correlate(d).cpu().numpy()
+    p = make_plan(chimex, E, F, T, algo=algo, tsplit=tsplit)
+    for _ in range(3):
+        out = p.correlate(d)
+        p.check_device()
+        np.testing.assert_array_equal(out.cpu().numpy(), want)
+    p.correlate(d, out, accumulate=True)
+    p.check_device()
+    np.testing.assert_array_equal(out.cpu().numpy(), (want.astype(np.int64) * 2).astype(np.int32))
+
+
 def test_offset_accumulate_and_preseed(chimex):
     T, F, E = 96, 3, 96
     packed = orc.generate(T, F, E, 4, 5, no_repeat=1)
