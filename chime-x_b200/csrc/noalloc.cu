@@ -16,8 +16,11 @@
 // the process exits.
 //
 // Limits: at most kNoAllocMaxChannels channels and kNoAllocMaxUnits work
-// units per call (for E = 2048 a channel needs 72 units, so up to 56 such
-// channels fit); larger requests are rejected with CHX_E_UNSUPPORTED.
+// units per call (for E = 2048 a channel needs 36 SM-pair units, so all 64
+// channels fit; E = 4096 needs 136); larger requests are rejected with
+// CHX_E_UNSUPPORTED.  The tile variant follows the plan path's default rule
+// (SM pair for an even number of 128-element tiles); sample ranges are cut
+// only where int32 exactness requires it.
 //
 // Sharing: every call, on every stream, uses the same array and leaves its
 // contents there.  Two calls whose kernels overlap on the GPU race on the
@@ -89,13 +92,18 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
     if (F > kNoAllocMaxChannels)
         return fail(CHX_E_UNSUPPORTED, "no-allocation entry point takes at most %d channels (F=%d)",
                     kNoAllocMaxChannels, F);
-    // Work units of the same shape as the plan-based path: per channel, each
-    // 128-element y tile against 256-element x ranges on and above the
-    // diagonal, sample ranges of at most kUnitMaxSamples.
-    const int nt = (E + 127) / 128;
+    // Work units of the same shape as the plan-based path's default tile:
+    // SM pair: 256-element y and x tile pairs on and above the diagonal;
+    // one SM: each 128-element y tile against 256-element x ranges; sample
+    // ranges of at most kUnitMaxSamples.
+    const int tile = tc_default_tile(E);
+    const int nt = (E + 127) / 128, nt2 = (nt + 1) / 2;
     const int chunks = (T + kUnitMaxSamples - 1) / kUnitMaxSamples;
     int64_t per_chan = 0;
-    for (int ty = 0; ty < nt; ty++) per_chan += (nt - ty + 1) / 2;
+    if (tile == kTile2Sm)
+        per_chan = (int64_t)nt2 * (nt2 + 1) / 2;
+    else
+        for (int ty = 0; ty < nt; ty++) per_chan += (nt - ty + 1) / 2;
     const int64_t nunits = per_chan * chunks * F;
     if (nunits > kNoAllocMaxUnits)
         return fail(CHX_E_UNSUPPORTED,
@@ -121,26 +129,36 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
     }
     Unit *units = g_host_sorted;
     int n = 0;
-    for (int f = 0; f < F; f++)
-        for (int ty = 0; ty < nt; ty++)
-            for (int x0 = ty; x0 < nt; x0 += 2)
-                for (int c = 0; c < chunks; c++) {
-                    Unit &u = units[n++];
+    auto add_unit = [&](int f, int tyx, int c, int cost_per_stage) {
+        Unit &u = units[n++];
+        u.chan = f;
+        u.tyx = tyx;
+        u.t0 = c * kUnitMaxSamples;
+        u.t1 = std::min(T, u.t0 + kUnitMaxSamples);
+        u.out_off = 0;
+        u.split = chunks > 1 ? 1 : 0;
+        u.cost = ((u.t1 - u.t0 + 31) / 32) * cost_per_stage;
+    };
+    for (int f = 0; f < F; f++) {
+        if (tile == kTile2Sm) {
+            for (int ty2 = 0; ty2 < nt2; ty2++)
+                for (int tx2 = ty2; tx2 < nt2; tx2++)
+                    for (int c = 0; c < chunks; c++) add_unit(f, ty2 | (tx2 << 10), c, 1);
+        } else {
+            for (int ty = 0; ty < nt; ty++)
+                for (int x0 = ty; x0 < nt; x0 += 2) {
                     const int nx = std::min(2, nt - x0);
-                    u.chan = f;
-                    u.tyx = ty | (x0 << 10) | (nx << 20);
-                    u.t0 = c * kUnitMaxSamples;
-                    u.t1 = std::min(T, u.t0 + kUnitMaxSamples);
-                    u.out_off = 0;
-                    u.split = chunks > 1 ? 1 : 0;
-                    u.cost = ((u.t1 - u.t0 + 31) / 32) * (nx + 1);
+                    for (int c = 0; c < chunks; c++)
+                        add_unit(f, ty | (x0 << 10) | (nx << 20), c, 2 * nx + 1);
                 }
+        }
+    }
     // Largest first, sorted in place (std::sort does not allocate), then dealt
     // round robin: CTA b takes sorted units b, b + grid, ... stored contiguously.
     std::sort(units, units + n, [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
     int sm_count = 0;
     CHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
-    const int grid = std::min(std::min(n, sm_count), kNoAllocMaxGrid);
+    const int grid = std::min(std::min(n, tc_tile_slots(tile, sm_count)), kNoAllocMaxGrid);
     Unit *dealt = reinterpret_cast<Unit *>(g_host_tables + kOffUnits);
     int *offsets = reinterpret_cast<int *>(g_host_tables + kOffOffsets);
     int k = 0;
@@ -180,6 +198,6 @@ extern "C" int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks,
     L.accumulate = accumulate ? 1 : 0;
     L.err = reinterpret_cast<int *>(dscr + kOffErr);
     L.grid = grid;
-    CHX_CUDA(tc_launch(L, &tmap, &omap, st));
+    CHX_CUDA(tc_tile_launch(tile, L, &tmap, &omap, st));
     return CHX_OK;
 }

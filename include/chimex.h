@@ -157,8 +157,10 @@ int chx_blocks_to_full(chx_plan *plan, const int32_t *d_blocks, int32_t *d_full,
  * This entry point computes exactly what chx_correlate computes for a plan
  * of (E, F, T, upper_triangle_convention), needs no plan and calls no
  * allocator: its work tables live in a fixed-size array inside the library
- * (about 162 KiB on every GPU that loads it, kept until exit).  Limits: F <= 64 channels and at
- * most 4096 work units (72 per E=2048 channel per 262144 samples); larger
+ * (about 162 KiB on every GPU that loads it, kept until exit).  It uses the
+ * plan path's default tile variant and cuts sample ranges only where int32
+ * exactness requires it (no automatic split).  Limits: F <= 64 channels and
+ * at most 4096 work units (36 per E=2048 channel per 262144 samples); larger
  * calls return CHX_E_UNSUPPORTED.  The first call on each device looks the
  * array up (and so loads the library's device code); make that first call
  * before any stream capture.  All calls share the array: calls whose kernels

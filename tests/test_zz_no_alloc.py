@@ -25,7 +25,7 @@ def test_noalloc_rejects_sizes_beyond_its_tables():
     rc = lib.chx_correlate_noalloc(fake, fake, 256, 65, 256, 1, 0, None)
     assert rc == chimex.E_UNSUPPORTED
     assert b"at most 64 channels" in lib.chx_last_error()
-    rc = lib.chx_correlate_noalloc(fake, fake, 2048, 60, 256, 1, 0, None)  # 60 x 72 units
+    rc = lib.chx_correlate_noalloc(fake, fake, 4096, 40, 256, 1, 0, None)  # 40 x 136 units
     assert rc == chimex.E_UNSUPPORTED
     assert b"work units" in lib.chx_last_error()
     assert lib.chx_correlate_noalloc(None, fake, 256, 1, 256, 1, 0, None) == chimex.E_INVALID
