@@ -6,6 +6,7 @@
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -162,8 +163,11 @@ void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets);
 // Makespan, in unit-cost units, of that assignment when every unit also pays
 // `handoff_stages` of its stages for the accumulator hand-off.
 long long tc_estimate_makespan(const std::vector<Unit> &u, int grid, int handoff_stages);
-// Number of sample-range splits (1-8) with the shortest estimated makespan
-// for F channels of E elements and T samples on the tile variant.
+// Number of sample-range splits k (1-8) whose units, made by build(k, out),
+// have the shortest estimated makespan on the tile variant.
+int tc_choose_split(int tile, int sm_count,
+                    const std::function<void(int, std::vector<Unit> &)> &build);
+// The same for F channels of E elements and T samples.
 int tc_auto_split(int tile, int E, int F, int T, int sm_count);
 // Encodes the TMA map of packed samples: dims {E, channels, samples}.
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,

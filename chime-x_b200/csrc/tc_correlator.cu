@@ -585,7 +585,8 @@ long long tc_estimate_makespan(const std::vector<Unit> &u, int grid, int handoff
     return span;
 }
 
-int tc_auto_split(int tile, int E, int F, int T, int sm_count) {
+int tc_choose_split(int tile, int sm_count,
+                    const std::function<void(int, std::vector<Unit> &)> &build) {
     // A unit's accumulator hand-off costs about as much as 11 of its stages in
     // the SM-pair kernel (measured on B200: ~9,400 cycles against ~850 per
     // stage) and about 16 in the one-SM kernel, whose unpack warps run the
@@ -598,17 +599,15 @@ int tc_auto_split(int tile, int E, int F, int T, int sm_count) {
     const int handoff_stages = tile == kTile2Sm ? 11 : 16;
     const int grid_slots = tc_tile_slots(tile, sm_count);
     long long best = -1;
-    int best_k = 1, last_chunks = 0;
+    int best_k = 1;
+    size_t last_n = 0;
     for (int k = 1; k <= 8; k++) {
         std::vector<Unit> units;
-        for (int f = 0; f < F; f++) tc_append_tile_units(tile, units, f, E, 0, T, k, 0);
+        build(k, units);
         if (units.empty()) return 1;
-        // Ranges are rounded to whole stages: skip counts that give the same cut.
-        const int chunks = (int)std::count_if(units.begin(), units.end(), [&](const Unit &x) {
-            return x.chan == 0 && x.tyx == units[0].tyx;
-        });
-        if (chunks == last_chunks) continue;
-        last_chunks = chunks;
+        // Ranges are rounded to whole stages: skip splits that cut the same way.
+        if (units.size() == last_n) continue;
+        last_n = units.size();
         const int grid = (int)std::min<size_t>(units.size(), (size_t)std::max(1, grid_slots));
         const long long span = tc_estimate_makespan(units, grid, handoff_stages);
         if (best < 0 || (k == 1 ? span < best : span * 100 < best * 97)) {
@@ -617,6 +616,12 @@ int tc_auto_split(int tile, int E, int F, int T, int sm_count) {
         }
     }
     return best_k;
+}
+
+int tc_auto_split(int tile, int E, int F, int T, int sm_count) {
+    return tc_choose_split(tile, sm_count, [&](int k, std::vector<Unit> &units) {
+        for (int f = 0; f < F; f++) tc_append_tile_units(tile, units, f, E, 0, T, k, 0);
+    });
 }
 
 int tc_encode_map(CUtensorMap *m, const void *base, int E, int channels, int64_t samples,
