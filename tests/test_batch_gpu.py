@@ -87,8 +87,8 @@ def test_ragged_batch_pair_tile(chimex):
 
 @pytest.mark.gpu
 def test_batch_split_integration(chimex):
-    # an integration above 2^18 samples is cut into split units that add
-    # atomically into zeroed outputs
+    # an integration above 2^18 samples is cut into split units that meet by
+    # TMA reduce-add in zeroed outputs
     specs = [(64, 300000, 1, 0), (32, 5, 1, 0)]
     b, chans, hosts = run_batch(chimex, specs, 1, seed=3)
     for accumulate, factor in ((False, 1), (True, 2)):
@@ -96,6 +96,25 @@ def test_batch_split_integration(chimex):
         b.check_device()
         for (E, T, nint, _), (packed, blocks, *_), host in zip(specs, chans, hosts):
             ref = oracle_blocks(host, E, T, nint, 1)
+            np.testing.assert_array_equal(blocks.cpu().numpy().reshape(nint, -1), factor * ref)
+
+
+@pytest.mark.gpu
+def test_batch_of_few_long_channels_is_split(chimex):
+    # two E=512 channels (three integrations) make only 9 SM-pair units for 74
+    # clusters: the batch splits their samples (8 ranges by the makespan
+    # estimate, 72 units), and the
+    # ranges of each tile pair meet by TMA reduce-add, twice in a row and in
+    # accumulate mode
+    specs = [(512, 4096, 1, 0), (512, 2000, 2, 0)]
+    b, chans, hosts = run_batch(chimex, specs, 1, seed=5)
+    assert b.work_units > 9
+    refs = [oracle_blocks(host, E, T, nint, 1)
+            for (E, T, nint, _), host in zip(specs, hosts)]
+    for accumulate, factor in ((False, 1), (False, 1), (True, 2)):
+        b.run(accumulate=accumulate)
+        b.check_device()
+        for (E, T, nint, _), (packed, blocks, *_), ref in zip(specs, chans, refs):
             np.testing.assert_array_equal(blocks.cpu().numpy().reshape(nint, -1), factor * ref)
 
 
