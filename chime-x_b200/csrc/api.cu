@@ -61,13 +61,15 @@ cudaError_t build_tc_tables(chx_plan *p) {
         chans[f].orow = (int)((int64_t)f * p->NB * 32);
     }
     std::vector<Unit> units;
-    // Unset options take the autotuner's cached choice for this shape, if any,
-    // else the default tile and no split.
+    // Unset options: the tile is the autotuner's cached choice for this shape,
+    // if any, else the default.  The tuned split was timed on a one-channel
+    // plan, so only a one-channel plan takes it; other plans split by the
+    // makespan estimate, which sees all of their units.
     int tile = p->tile, split = p->tsplit;
     int tuned_tile = 0, tuned_split = 0;
     if ((!tile || !split) && tc_tune_lookup(p->device, p->E, p->T, &tuned_tile, &tuned_split)) {
         if (!tile) tile = tuned_tile;
-        if (!split) split = tuned_split;
+        if (!split && p->F == 1) split = tuned_split;
     }
     if (!tile) tile = tc_default_tile(p->E);
     if (!split) split = tc_auto_split(tile, p->E, p->F, p->T, p->sm_count);

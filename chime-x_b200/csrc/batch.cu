@@ -184,23 +184,17 @@ int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int 
                   ? tv.tile
                   : tc_default_tile(descs[heaviest].num_elements);
 
-    // Sample splits: the autotuned one where the cache has the channel's shape,
-    // else one split for all other channels, chosen for the whole batch by
-    // the makespan estimate (a few long channels are split to fill the GPU;
-    // many short integrations are not).
-    std::vector<int> tuned_split(n, 0);
-    for (int c = 0; c < n; c++) {
-        TuneVal tc;
-        if (tune_lookup(device, descs[c].num_elements, descs[c].num_timesamples, &tc))
-            tuned_split[c] = tc.split;
-    }
+    // Sample splits: one for every channel, chosen for the whole batch by the
+    // makespan estimate (a few long channels are split to fill the GPU, many
+    // short integrations are not).  The autotuner's split was timed on a lone
+    // channel, where splitting fills idle SMs that a batch already fills, so
+    // batches take only its tile.
     const int auto_split = tc_choose_split(b->tile, sm_count, [&](int k, std::vector<Unit> &u) {
         for (int c = 0; c < n; c++)
             for (int i = 0; i < descs[c].num_integrations; i++)
                 tc_append_tile_units(b->tile, u, c, descs[c].num_elements,
                                      i * descs[c].num_timesamples,
-                                     (i + 1) * descs[c].num_timesamples,
-                                     tuned_split[c] ? tuned_split[c] : k, 0);
+                                     (i + 1) * descs[c].num_timesamples, k, 0);
     });
 
     std::vector<ChanDesc> chans(n);
@@ -227,7 +221,7 @@ int chx_batch_create(chx_batch **out, int n, const chx_channel_desc *descs, int 
         chans[c].E = d.num_elements;
         chans[c].nb1 = d.num_elements / 32;
         chans[c].fcoord = 0;
-        const int split = tuned_split[c] ? tuned_split[c] : auto_split;
+        const int split = auto_split;
         const int64_t nb = num_blocks_of(d.num_elements);
         for (int i = 0; i < d.num_integrations; i++) {
             const size_t before = units.size();

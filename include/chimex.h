@@ -202,8 +202,10 @@ typedef struct chx_channel_desc {
 typedef struct chx_batch chx_batch;
 
 /* Builds the tile queue for n channels.  The descriptors are copied.  The
- * channel work is ordered by a cost model; tile variant and sample splits
- * come from the autotuner's cache (chx_autotune) when present. */
+ * channel work is ordered by a cost model.  The tile variant is the
+ * autotuner's (chx_autotune) for the costliest channel when cached, else the
+ * default; the sample split is one for the whole batch, chosen by a makespan
+ * estimate so that a few long channels still fill the GPU. */
 int chx_batch_create(chx_batch **batch, int n, const chx_channel_desc *descs,
                      int upper_triangle_convention, int device);
 /* Enqueues the whole batch (one graph launch).  accumulate as chx_correlate. */
@@ -216,10 +218,13 @@ double chx_batch_ops(const chx_batch *batch);
 int chx_batch_check(chx_batch *batch, void *stream);
 int chx_batch_destroy(chx_batch *batch);
 
-/* Times the tensor-core tile variants and split counts for (E, T) on the
- * current device and caches the winner: batches and plans created afterwards
- * (with CHX_OPT_TILE / CHX_OPT_TSPLIT left at 0) take it for channels of the
- * same E and a T within a factor 2.
+/* Times the tensor-core tile variants and split counts for a one-channel
+ * plan of (E, T) on the current device and caches the winner.  Batches and
+ * plans created afterwards with CHX_OPT_TILE left at 0 take its tile for
+ * channels of the same E and a T within a factor 2; one-channel plans with
+ * CHX_OPT_TSPLIT left at 0 take its split as well (other plans and batches
+ * split by their own makespan estimate, since the best split depends on how
+ * many units the whole launch has).
  * d_scratch_in/d_scratch_out must hold T*E bytes and NB*2048 int32. */
 int chx_autotune(int num_elements, int num_timesamples, const uint8_t *d_scratch_in,
                  int32_t *d_scratch_out, void *stream, int *best_tile,

@@ -193,7 +193,7 @@ def test_autotune_choice_is_exact(chimex):
     out = torch.empty(orc.num_blocks(E) * 2048, dtype=torch.int32, device="cuda")
     tile, split, ms = cx.autotune(E, T, x, out)
     assert tile in (1, 2) and split in (1, 2, 4) and ms > 0
-    # a batch of this shape now uses the tuned tile and split
+    # a batch of this shape now uses the tuned tile (its own split)
     blocks = torch.full_like(out, -7)
     b = cx.Batch([(x, blocks, E, T, 1)])
     b.run()
