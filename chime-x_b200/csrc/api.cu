@@ -62,15 +62,13 @@ cudaError_t build_tc_tables(chx_plan *p) {
     }
     std::vector<Unit> units;
     // Unset options: the tile is the autotuner's cached choice for this shape,
-    // if any, else the default.  The tuned split was timed on a one-channel
-    // plan, so only a one-channel plan takes it; other plans split by the
-    // makespan estimate, which sees all of their units.
+    // if any, else the default; the split comes from the makespan estimate,
+    // which sees how many units this plan has (the tuner times a workload that
+    // fills the GPU, where splitting only adds hand-offs).
     int tile = p->tile, split = p->tsplit;
     int tuned_tile = 0, tuned_split = 0;
-    if ((!tile || !split) && tc_tune_lookup(p->device, p->E, p->T, &tuned_tile, &tuned_split)) {
-        if (!tile) tile = tuned_tile;
-        if (!split && p->F == 1) split = tuned_split;
-    }
+    if (!tile && tc_tune_lookup(p->device, p->E, p->T, &tuned_tile, &tuned_split))
+        tile = tuned_tile;
     if (!tile) tile = tc_default_tile(p->E);
     if (!split) split = tc_auto_split(tile, p->E, p->F, p->T, p->sm_count);
     for (int f = 0; f < p->F; f++) tc_append_tile_units(tile, units, f, p->E, 0, p->T, split, 0);

@@ -330,9 +330,49 @@ int chx_autotune(int E, int T, const uint8_t *d_in, int32_t *d_out, void *stream
     int dev = 0;
     CHX_CUDA(cudaGetDevice(&dev));
     cudaStream_t st = (cudaStream_t)stream;
+    // Channels timed together: enough for about two waves of SM-pair units,
+    // so that the comparison measures each variant's speed per unit rather
+    // than how many SMs a lone channel leaves idle (a lone E=2048 channel has
+    // 36 SM-pair units for 74 clusters).  The caller's scratch holds one
+    // channel; more come from a temporary allocation (at most 64 channels
+    // and 2 GiB), without which the lone channel is timed.
+    int sm_count = 0;
+    CHX_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
+    if (E < 32 || E % 32 != 0 || T < 1) return fail(CHX_E_INVALID, "E=%d T=%d", E, T);
+    const int64_t nt2 = ((E + 127) / 128 + 1) / 2;
+    const int64_t pair_units = nt2 * (nt2 + 1) / 2;
+    const int64_t nb = num_blocks_of(E);
+    int64_t F = std::min<int64_t>(64, std::max<int64_t>(1, (sm_count + pair_units - 1) / pair_units));
+    while (F > 1 && F * ((int64_t)T * E + nb * 2048 * 4) > (2LL << 30)) F--;
+    const uint8_t *in = d_in;
+    int32_t *out = d_out;
+    void *own_in = nullptr, *own_out = nullptr;
+    if (F > 1) {
+        if (cudaMalloc(&own_in, (size_t)F * T * E) != cudaSuccess ||
+            cudaMalloc(&own_out, (size_t)F * nb * 2048 * 4) != cudaSuccess) {
+            cudaGetLastError();  // out of memory: time the lone channel instead
+            if (own_in) cudaFree(own_in);
+            own_in = own_out = nullptr;
+            F = 1;
+        } else {
+            // The kernels' speed does not depend on the sample values.
+            const cudaError_t me = cudaMemsetAsync(own_in, 0x5a, (size_t)F * T * E, st);
+            if (me != cudaSuccess) {
+                cudaFree(own_in);
+                cudaFree(own_out);
+                return cuda_fail(me, "autotune scratch");
+            }
+            in = static_cast<const uint8_t *>(own_in);
+            out = static_cast<int32_t *>(own_out);
+        }
+    }
     chx_plan *p = nullptr;
-    int rc = chx_plan_create(&p, E, 1, T, T, 1, 0, dev);
-    if (rc != CHX_OK) return rc;
+    int rc = chx_plan_create(&p, E, (int)F, T, T, 1, 0, dev);
+    if (rc != CHX_OK) {
+        if (own_in) cudaFree(own_in);
+        if (own_out) cudaFree(own_out);
+        return rc;
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t ce = cudaEventCreate(&e0);
     if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
@@ -345,10 +385,10 @@ int chx_autotune(int E, int T, const uint8_t *d_in, int32_t *d_out, void *stream
             rc = chx_plan_set_option(p, CHX_OPT_TILE, tiles[ti]);
             if (rc == CHX_OK) rc = chx_plan_set_option(p, CHX_OPT_TSPLIT, splits[si]);
             if (rc != CHX_OK) break;
-            for (int w = 0; w < 2 && rc == CHX_OK; w++) rc = chx_correlate(p, d_in, d_out, st, 0);
+            for (int w = 0; w < 2 && rc == CHX_OK; w++) rc = chx_correlate(p, in, out, st, 0);
             const int reps = 5;
             ce = cudaEventRecord(e0, st);
-            for (int r = 0; r < reps && rc == CHX_OK; r++) rc = chx_correlate(p, d_in, d_out, st, 0);
+            for (int r = 0; r < reps && rc == CHX_OK; r++) rc = chx_correlate(p, in, out, st, 0);
             if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
             if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
             float ms = 0;
@@ -361,6 +401,8 @@ int chx_autotune(int E, int T, const uint8_t *d_in, int32_t *d_out, void *stream
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     chx_plan_destroy(p);
+    if (own_in) cudaFree(own_in);
+    if (own_out) cudaFree(own_out);
     if (rc != CHX_OK) return rc;
     if (ce != cudaSuccess) return cuda_fail(ce, "autotune timing");
     {

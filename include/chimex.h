@@ -218,13 +218,15 @@ double chx_batch_ops(const chx_batch *batch);
 int chx_batch_check(chx_batch *batch, void *stream);
 int chx_batch_destroy(chx_batch *batch);
 
-/* Times the tensor-core tile variants and split counts for a one-channel
- * plan of (E, T) on the current device and caches the winner.  Batches and
- * plans created afterwards with CHX_OPT_TILE left at 0 take its tile for
- * channels of the same E and a T within a factor 2; one-channel plans with
- * CHX_OPT_TSPLIT left at 0 take its split as well (other plans and batches
- * split by their own makespan estimate, since the best split depends on how
- * many units the whole launch has).
+/* Times the tensor-core tile variants and split counts for channels of
+ * (E, T) on the current device and caches the winner.  It times enough
+ * channels to fill the GPU (about two waves of SM-pair units; beyond the one
+ * channel the caller's scratch holds it allocates temporary buffers, up to 64
+ * channels and 2 GiB), so the choice reflects each variant's speed rather
+ * than how many SMs a lone channel leaves idle.  Batches and plans created
+ * afterwards with CHX_OPT_TILE left at 0 take its tile for channels of the
+ * same E and a T within a factor 2.  Their sample split comes from their own
+ * makespan estimate, which sees how many units the whole launch has.
  * d_scratch_in/d_scratch_out must hold T*E bytes and NB*2048 int32. */
 int chx_autotune(int num_elements, int num_timesamples, const uint8_t *d_scratch_in,
                  int32_t *d_scratch_out, void *stream, int *best_tile,

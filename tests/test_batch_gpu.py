@@ -202,7 +202,7 @@ def test_autotune_choice_is_exact(chimex):
     p.set_option(cx.OPT_ALGO, cx.ALGO_SIMT)
     ref = p.correlate(x)
     assert torch.equal(blocks, ref)
-    # a plan of this shape created now takes the tuned tile and split too
+    # a plan of this shape created now takes the tuned tile too
     q = cx.Plan(E, 1, T, T)
     assert torch.equal(q.correlate(x), ref)
     q.check_device()
