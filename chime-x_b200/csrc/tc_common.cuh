@@ -142,15 +142,6 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
         : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-}
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
@@ -176,21 +167,10 @@ __device__ __forceinline__ void sts128(uint32_t addr, uint32_t a, uint32_t b, ui
                  : "memory");
 }
 
-// Writes one row (lane) of a 32 x 32-word staging tile: 16 (Re, Im) pairs
-// as eight 16-byte chunks, chunk c at position c ^ (row & 7) (the 128-byte
-// swizzle of the output tensor map), so the warp's stores hit every bank.
-__device__ __forceinline__ void stage_row(uint32_t tile, int row, const uint32_t (&re)[16],
-                                          const uint32_t (&im)[16]) {
-    const uint32_t base = tile + (uint32_t)row * 128u;
-    const uint32_t x = (uint32_t)(row & 7);
-#pragma unroll
-    for (int c = 0; c < 8; c++)
-        sts128(base + (((uint32_t)c ^ x) << 4), re[2 * c], im[2 * c], re[2 * c + 1],
-               im[2 * c + 1]);
-}
-
-// Half of a staging row: (Re, Im) pairs 8*part .. 8*part+7 as chunks
-// 4*part .. 4*part+3 (same swizzle as stage_row).
+// Half of one row (lane) of a 32 x 32-word staging tile: (Re, Im) pairs
+// 8*part .. 8*part+7 as the 16-byte chunks 4*part .. 4*part+3, chunk c at
+// position c ^ (row & 7) (the 128-byte swizzle of the output tensor map), so
+// the warp's stores spread over every bank.
 __device__ __forceinline__ void stage_row_half(uint32_t tile, int row, int part,
                                                const uint32_t (&re)[8], const uint32_t (&im)[8]) {
     const uint32_t base = tile + (uint32_t)row * 128u;
