@@ -605,6 +605,9 @@ int tc_choose_split(int tile, int sm_count,
         std::vector<Unit> units;
         build(k, units);
         if (units.empty()) return 1;
+        // Eight or more waves of unsplit units leave at most about an eighth
+        // of a wave idle, less than the hand-offs that splitting adds.
+        if (k == 1 && units.size() >= (size_t)8 * std::max(1, grid_slots)) return 1;
         // Ranges are rounded to whole stages: skip splits that cut the same way.
         if (units.size() == last_n) continue;
         last_n = units.size();
