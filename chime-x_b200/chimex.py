@@ -296,9 +296,11 @@ class Plan:
 
 
 def autotune(E, T, scratch_in, scratch_out, stream=None):
-    """Times the tile variants and sample splits for (E, T) on the current
-    device (chx_autotune); returns (tile, split, ms) and caches the winner for
-    later batches."""
+    """Times the tile variants and sample splits for channels of (E, T) on the
+    current device (chx_autotune), on enough channels to fill the GPU (it
+    allocates temporary buffers beyond the one channel of scratch given);
+    returns (tile, split, ms) and caches the tile for later plans and
+    batches, which choose their own split."""
     tile, split, ms = _i(), _i(), ctypes.c_double()
     check(_lib.chx_autotune(E, T, _ptr(scratch_in), _ptr(scratch_out), _stream(stream),
                             ctypes.byref(tile), ctypes.byref(split), ctypes.byref(ms)))
