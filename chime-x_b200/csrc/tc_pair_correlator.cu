@@ -47,7 +47,7 @@ using namespace tc;
 constexpr int kStageSamples = 32;
 constexpr int kOpSlots = 4;     // 2 stage pairs
 constexpr int kPairs = kOpSlots / 2;
-constexpr int kPkStages = 8;
+constexpr int kPkStages = 4;
 constexpr int kYOpBytes = 16 * 1024;
 constexpr int kXOpBytes = 8 * 1024;
 constexpr int kPkBytes = kStageSamples * 128;  // one 128-element tile, 4 KiB
@@ -56,7 +56,7 @@ constexpr int kProducerWarp = 16;
 constexpr int kMmaWarp = 17;
 constexpr int kEpiWarp0 = 18;   // epilogue warps from here on, lane quarter = warp % 4
 constexpr int kEpiWarps = 8;    // 4 or 8: each warp drains 8 / (kEpiWarps / 4) column blocks
-constexpr int kEpiTiles = 2;    // 4 KiB output staging tiles per epilogue warp
+constexpr int kEpiTiles = 3;    // 4 KiB output staging tiles per epilogue warp
 constexpr int kEpiStageBytes = kEpiTiles * 4096;
 constexpr int kEpiBlocks = 8 / (kEpiWarps / 4);
 constexpr int kThreads = (kEpiWarp0 + kEpiWarps) * 32;
