@@ -1,0 +1,54 @@
+"""Host-side arithmetic of bench.py (no GPU): the work and real-time-channel
+conversions, the roofline denominator, the DRAM traffic read from the committed
+ncu summaries, and the rule that the product package never reaches the CPU
+oracle."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+import bench  # noqa: E402
+
+
+def test_exact_ops_and_realtime_channel():
+    # 8 ops (4 int8 MACs) per upper-triangle complex visibility per sample
+    assert bench.vis_ops(2048, 1, 1) == 8 * 2048 * 2049 / 2
+    assert bench.vis_ops(256, 10, 3) == 3 * 10 * bench.vis_ops(256, 1, 1)
+    # one real-time E=2048 channel is 390625 samples/s of that work: 6.557 TOPS
+    assert bench.E2048_RT_TOPS == pytest.approx(bench.vis_ops(2048, 390625, 1) / 1e12)
+    assert bench.E2048_RT_TOPS == pytest.approx(6.557, abs=1e-3)
+
+
+def test_int8_peak_is_twice_the_measured_bf16_burst():
+    peak, src = bench.int8_peak({"bf16_tflops": 1691.3, "hbm_gbs": 6452.8})
+    assert peak == pytest.approx(3382.6)
+    assert "measured" in src
+    peak, src = bench.int8_peak(None)
+    assert peak == pytest.approx(3180.0)
+    assert "fallback" in src
+
+
+def test_traffic_comes_from_the_committed_summaries():
+    plain = bench.profile_traffic("tc_pair_correlate_E2048_F8_T16384.md")
+    batched = bench.profile_traffic("tc_pair_correlate_batched64.md")
+    # both captures moved about the algorithmic bytes (input once, blocks once)
+    assert plain is not None and 0.9 < plain / (268435456 + 136314880) < 1.2
+    assert batched is not None and 0.9 < batched / (314327040 + 1816395776) < 1.1
+    assert bench.profile_traffic("no_such_summary.md") is None
+
+
+def test_product_package_does_not_reach_the_oracle():
+    pkg = os.path.join(ROOT, "chime-x_b200")
+    offenders = []
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if not f.endswith((".py", ".cu", ".cuh", ".h", ".c", ".cpp")):
+                continue
+            with open(os.path.join(dirpath, f), errors="replace") as fh:
+                text = fh.read()
+            if "oracle" in text or "pyoracle" in text or "chx_oracle" in text:
+                offenders.append(os.path.relpath(os.path.join(dirpath, f), ROOT))
+    assert offenders == []
