@@ -1,28 +1,42 @@
 """Benchmark of the CHIME X-engine hot path on B200.
 
-Default workload (N=1): the plain correlator at full CHIME size, E=2048
+Headline workload (N=1): the plain correlator at full CHIME size, E=2048
 elements, F=8 channels, T=16384 samples (64 integrations of time_accum=256),
 one fused chx_correlate launch per step over inputs already resident in HBM.
 Metric: exact INT8 tensor-core TOPS = 8 * E(E+1)/2 * T * F / seconds (4 int8
 MACs per upper-triangle complex visibility per sample; diagonal-tile waste
 not credited).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--config plain|batched|stream|helpers] [--algo auto|simt|tc]
+The default run prints ONE JSON line holding, besides the headline value:
+  sustained         >= 5 s of back-to-back launches of the same workload with
+                    the SM clock sampled, binned by clock; real-time channels
+  int8_peak_in_run  a cuBLAS int8 GEMM (torch._int_mm, 8192^3) timed in the
+                    same process, with its median SM clock
+  batched           BASELINE config 4: 64 ragged channels in one CUDA-graph
+                    launch against the plain per-channel launches
+  stream            BASELINE config 5: 1024-channel streaming loop, real-time
+                    channels sustained, p50/p99 frame-to-visibility latency
+  e2e, cpu_baseline, roofline, clocks, gpu_launches
 
-Under torchrun each rank correlates its own F channels (weak scaling, no
-data-path collective); the time is the max over ranks.  `--impl reference`
-times the reference's own CPU correlator (cpu_corr_test.c, built from the
-reference sources into oracle/_ref) on the host cores instead.
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--config all|plain|batched|stream|helpers] [--algo auto|simt|tc]
+
+Multi-GPU: one process per GPU.  `--gpus N` without a torchrun environment
+relaunches itself under torch.distributed.run.  Each rank correlates its own
+plain-workload channels (weak scaling) and its share of the batched and
+streamed channel lists (largest-first assignment, strong scaling); there is
+no data-path collective, the job time is the max over ranks and the work the
+sum over ranks.  `--impl reference` times the reference's own CPU correlator
+(cpu_corr_test.c, built from the reference sources into oracle/_ref) on the
+host cores instead.
 """
 import argparse
-import ctypes
 import json
 import os
 import statistics
 import subprocess
 import sys
-import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -66,6 +80,23 @@ def env_rank():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def shard_channels(costs, world, rank):
+    """Indices of the channels rank `rank` owns out of `world` ranks: the
+    channels, costliest first (ties by index), each go to the rank with the
+    least cost so far (ties to the lowest rank).  Deterministic, so every rank
+    computes the same partition without communicating: the shards are
+    disjoint and cover every channel."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += costs[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
 # ----------------------------------------------------------------- peaks
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -103,37 +134,96 @@ def profile_traffic(name):
     return None
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 # ----------------------------------------------------------------- clocks
+# NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*).
+_REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+REJECT_REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                  "hw_power_brake_slowdown")
+
+
 class ClockSampler:
-    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+    """Samples the SM clock, power and clock-event reasons of one GPU through
+    NVML from a background thread every `period_s` (2 ms by default: fine
+    enough to see a 20 ms timed region).  Reading only: nothing is set."""
 
-    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    def __init__(self, torch_device, period_s=0.002):
+        self.dev = torch_device
+        self.period = period_s
+        self.samples = []  # (time, sm MHz, power W, reasons bits)
+        self.handle = None
+        self.nvml = None
+        self.sm_max = None
+        self._stop = threading.Event()
+        self._thread = None
+        self.t0 = self.t1 = None
+        self.error = None
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.tmp = None
+    def _open(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.dev)
+        h = None
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+        except Exception:
+            h = None
+        if h is None:
+            try:
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(
+                    "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id,
+                                          props.pci_device_id))
+            except Exception:
+                h = None
+        if h is None:
+            h = pynvml.nvmlDeviceGetHandleByIndex(int(self.dev.index or 0))
+        self.nvml, self.handle = pynvml, h
+        self.sm_max = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+    def _run(self):
+        nv, h = self.nvml, self.handle
+        while not self._stop.is_set():
+            try:
+                t = time.time()
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((t, sm, pw, rs))
+            except Exception as e:  # keep the benchmark running without clocks
+                self.error = str(e)
+                return
+            time.sleep(self.period)
 
     def __enter__(self):
         try:
-            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=self.tmp, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            self._open()
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        except Exception as e:
+            self.error = "nvml unavailable: %s" % e
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+        try:
+            if self.nvml is not None:
+                self.nvml.nvmlShutdown()
+        except Exception:
+            pass
 
     def mark_start(self):
         self.t0 = time.time()
@@ -141,63 +231,56 @@ class ClockSampler:
     def mark_end(self):
         self.t1 = time.time()
 
-    def summary(self):
-        if self.proc is None or self.tmp is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.tmp.flush()
-        rows = []
-        with open(self.tmp.name) as fh:
-            for line in fh:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.tmp.name)
-        import datetime
-        t0, t1 = getattr(self, "t0", None), getattr(self, "t1", None)
-        if t0 is not None and t1 is not None:
-            keep = []
-            for r in rows:
-                try:
-                    ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                except ValueError:
-                    continue
-                if t0 - 0.05 <= ts <= t1 + 0.05:
-                    keep.append(r)
-            rows = keep
+    def window(self, t0=None, t1=None):
+        t0 = self.t0 if t0 is None else t0
+        t1 = self.t1 if t1 is None else t1
+        if t0 is None or t1 is None:
+            return list(self.samples)
+        return [s for s in self.samples if t0 <= s[0] <= t1]
+
+    def summary(self, t0=None, t1=None):
+        rows = self.window(t0, t1)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        def num(x):
-            try:
-                return float(x)
-            except ValueError:
-                return None
-        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
-        smax = [num(r[2]) for r in rows if num(r[2]) is not None]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = []
-        for k, n in enumerate(names):
-            if any(r[5 + k].lower().startswith("active") for r in rows):
-                reasons.append(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "power_w_max": max((num(r[3]) or 0.0) for r in rows),
-                "samples": len(rows), "reasons": reasons}
+            return {"sm_mhz": None, "sm_max_mhz": self.sm_max,
+                    "reasons": [self.error or "no samples"], "samples": 0}
+        sm = [r[1] for r in rows]
+        reasons = [n for n, bit in _REASONS.items() if any(r[3] & bit for r in rows)]
+        return {"sm_mhz": statistics.median(sm), "sm_min_mhz": min(sm),
+                "sm_max_mhz": self.sm_max, "power_w_max": max(r[2] for r in rows),
+                "samples": len(rows), "reasons": reasons, "source": "NVML, 2 ms"}
+
+
+def clocks_rejected(summary):
+    """True when a clock record shows a throttle that invalidates a number
+    (hardware or thermal slowdown), or SM clocks stuck well below the maximum
+    with no reason (a leftover clock lock)."""
+    if any(r in REJECT_REASONS for r in summary.get("reasons", [])):
+        return True
+    sm, smax = summary.get("sm_mhz"), summary.get("sm_max_mhz")
+    if sm and smax and sm < 0.8 * smax and not summary.get("reasons"):
+        return True
+    return False
 
 
 # ------------------------------------------------------------ cpu baseline
-def cpu_reference_rate(E, T_sample, seconds_target=12.0, max_procs=None):
+def _ref_driver():
+    p = os.path.join(ROOT, "oracle", "_ref", "cpu_corr_ref")
+    return p if os.path.exists(p) else None
+
+
+def cpu_reference_rate(E, T_sample, max_procs=None, no_repeat=1, seed0=42):
     """Times the reference's own CPU correlator (oracle/_ref/cpu_corr_ref,
     built from cpu_corr_test.c) on the host cores: one process per core, each
     correlating one E-element channel over T_sample samples.  Returns
-    (ops_per_s, cores, sample description, kind)."""
-    driver = os.path.join(ROOT, "oracle", "_ref", "cpu_corr_ref")
-    kind = "reference"
-    if not os.path.exists(driver):
+    (ops_per_s, cores, sample description, kind, wall seconds) or None."""
+    driver = _ref_driver()
+    if driver is None:
         return None
     cores = max_procs or os.cpu_count() or 1
     t0 = time.time()
-    procs = [subprocess.Popen([driver, str(T_sample), "1", str(E), "4", str(42 + i), "1", "1"],
-                              stdout=subprocess.PIPE, text=True) for i in range(cores)]
+    procs = [subprocess.Popen([driver, str(T_sample), "1", str(E), "4", str(seed0 + i),
+                               str(no_repeat), "1"], stdout=subprocess.PIPE, text=True)
+             for i in range(cores)]
     outs = [p.communicate()[0] for p in procs]
     wall = time.time() - t0
     total_ops = 0.0
@@ -206,7 +289,37 @@ def cpu_reference_rate(E, T_sample, seconds_target=12.0, max_procs=None):
         total_ops += OPS_PER_VIS_SAMPLE * rec["updates"]
     sample = ("%d concurrent processes x (E=%d, F=1, T=%d, seeded random) of the "
               "reference cpu_data_generate_and_correlate_upper_triangle_only" % (cores, E, T_sample))
-    return total_ops / wall, cores, sample, kind, wall
+    return total_ops / wall, cores, sample, "reference", wall
+
+
+def cpu_single_core():
+    """The reference CPU correlator on ONE core: BASELINE config 1 in full
+    (E=256, F=1, T=256, seed 42, repeating generator), repeated for about a
+    second, and a bounded sample of config 2 (E=2048, F=1, T=512, no repeat).
+    Each figure is the reference's own timing of its correlation loop."""
+    driver = _ref_driver()
+    if driver is None:
+        return None
+    out = {"cores": 1, "cpu_model": cpu_model(), "kind": "reference"}
+
+    def run(T, E, no_repeat):
+        r = subprocess.run([driver, str(T), "1", str(E), "4", "42", str(no_repeat), "1"],
+                           capture_output=True, text=True, check=True)
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    recs, t_end = [], time.time() + 1.0
+    while time.time() < t_end or not recs:
+        recs.append(run(256, 256, 0))
+    secs = statistics.median(r["seconds"] for r in recs)
+    out["config1"] = {"value": OPS_PER_VIS_SAMPLE * recs[0]["updates"] / secs / 1e12,
+                      "unit": "TOPS", "seconds": secs, "runs": len(recs),
+                      "sample": "E=256 F=1 T=256 seed 42 repeat (config 1 in full)",
+                      "triangle_fnv": recs[0]["hash"]}
+    r2 = run(512, 2048, 1)
+    out["config2_sample"] = {"value": OPS_PER_VIS_SAMPLE * r2["updates"] / r2["seconds"] / 1e12,
+                             "unit": "TOPS", "seconds": r2["seconds"],
+                             "sample": "E=2048 F=1 T=512 seed 42 no repeat (1/256 of config 2)"}
+    return out
 
 
 def run_reference_arm(args):
@@ -214,8 +327,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     E, F, T = 2048, 8, 16384
-    driver = os.path.join(ROOT, "oracle", "_ref", "cpu_corr_ref")
-    if not os.path.exists(driver):
+    if _ref_driver() is None:
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/cpu_corr_ref not built (needs the reference sources)"}))
         return 0
@@ -244,6 +356,7 @@ def run_reference_arm(args):
         "config": {"workload": "plain correlator E=2048 F=8 T=16384 time_accum=256; each step "
                                "a bounded sample of it on the host cores", "E": E, "F": F, "T": T},
         "cpu_baseline": {"value": value, "unit": "TOPS", "cores": cores, "kind": "reference",
+                         "cpu_model": cpu_model(),
                          "sample": "%d processes x (E=%d, T=%d) per step" % (cores, E, t_sample)},
         "e2e": {"value": value, "unit": "TOPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "realtime_channels_e2048": ops_s / (E2048_RT_TOPS * 1e12),
@@ -253,11 +366,8 @@ def run_reference_arm(args):
 
 
 # --------------------------------------------------------------- our arm
-def run_plain(args, torch, cx, dist):
-    rank, local_rank, world = env_rank()
-    E, F, T, TA = args.E, args.F, args.T, 256
-    dev = torch.device("cuda", local_rank)
-    plan = cx.Plan(E, F, T, TA, 1, 0, local_rank)
+def make_plain_plan(args, cx, local_rank):
+    plan = cx.Plan(args.E, args.F, args.T, 256, 1, 0, local_rank)
     if args.algo == "simt":
         plan.set_option(cx.OPT_ALGO, cx.ALGO_SIMT)
     elif args.algo == "tc":
@@ -266,6 +376,15 @@ def run_plain(args, torch, cx, dist):
         plan.set_option(cx.OPT_TSPLIT, args.tsplit)
     if args.tile:
         plan.set_option(cx.OPT_TILE, args.tile)
+    return plan
+
+
+def run_plain(args, torch, cx, dist, clk):
+    """The headline leg: one chx_correlate launch of config 2 per step."""
+    rank, local_rank, world = env_rank()
+    E, F, T, TA = args.E, args.F, args.T, 256
+    dev = torch.device("cuda", local_rank)
+    plan = make_plain_plan(args, cx, local_rank)
     gen = torch.Generator(device=dev)
     gen.manual_seed(42 + rank)
     packed = torch.randint(0, 256, (plan.input_bytes,), dtype=torch.uint8, device=dev,
@@ -277,58 +396,40 @@ def run_plain(args, torch, cx, dist):
     def step():
         plan.correlate(packed, blocks, stream=stream)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
-    with ClockSampler(local_rank) as clk:
-        for _ in range(max(args.warmup, 3)):
-            step()
-        plan.check_device()
-        torch.cuda.synchronize(dev)
-        # device-timed region: inputs larger than L2 (see config["l2"])
-        barrier()
-        torch.cuda.synchronize(dev)
-        clk.mark_start()
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        t_start.record(stream)
-        for k in range(args.steps):
-            ev[k][0].record(stream)
-            step()
-            ev[k][1].record(stream)
-        t_end.record(stream)
-        torch.cuda.synchronize(dev)
-        clk.mark_end()
-    barrier()
+    for _ in range(max(args.warmup, 3)):
+        step()
     plan.check_device()
-    total_ms = t_start.elapsed_time(t_end)
-    per_launch = [a.elapsed_time(b) for a, b in ev]
-    total_ms = max_over_ranks(total_ms, dist, dev)
-    value = ops_step * world * args.steps / (total_ms * 1e-3) / 1e12
+    torch.cuda.synchronize(dev)
+    # device-timed region: inputs larger than L2 (see config["l2"])
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    clk.mark_start()
+    t_start.record(stream)
+    for k in range(args.steps):
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    clk.mark_end()
+    if dist is not None:
+        dist.barrier()
+    plan.check_device()
     clocks = clk.summary()
-
-    # end to end through the public API with host buffers: pinned input
-    # copied H2D and the block buffer copied D2H every step, two stages
-    # double-buffered on two streams (main_wrapper.c:614-785 style).
-    e2e = None
-    if not args.no_e2e:
-        e2e = run_e2e(args, torch, cx, plan, dev, ops_step, world, dist)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_reference_rate(E, 3072)
-        if r is not None:
-            cpu = {"value": r[0] / 1e12, "unit": "TOPS", "cores": r[1], "kind": r[3],
-                   "sample": r[2], "seconds": round(r[4], 2)}
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end), dist, dev)
+    per_launch = [a.elapsed_time(b) for a, b in ev]
+    job_ops = sum_over_ranks(ops_step * args.steps, dist, dev)
+    value = job_ops / (total_ms * 1e-3) / 1e12
 
     peak, peak_src = int8_peak(load_peaks())
     traffic = None
     if (E, F, T) == (2048, 8, 16384) and args.algo != "simt" and args.tile in (0, 2):
         traffic = profile_traffic("tc_pair_correlate_E2048_F8_T16384.md")
-    kernel_ms = sorted(per_launch)[len(per_launch) // 2]
     achieved = ops_step / (sum(per_launch) / len(per_launch) * 1e-3) / 1e12
     line = {
         "metric": "exact INT8-TC TOPS", "value": value, "unit": "TOPS", "n_gpus": world,
@@ -336,31 +437,136 @@ def run_plain(args, torch, cx, dist):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
         "data": "synthetic: seeded uniform 4-bit complex (re, im uniform in [-8, 7]), "
                 "device-generated",
-        "config": {"workload": "plain correlator E=%d F=%d T=%d time_accum=256 per GPU, "
-                               "one chx_correlate launch per step" % (E, F, T),
+        "config": {"workload": "Plain correlator at full CHIME size: E=2048, F=8, T=16384 "
+                               "(64 integrations of time_accum=256), random uniform [-8,7] "
+                               "re/im; one chx_correlate launch per step per GPU",
                    "E": E, "F": F, "T": T, "time_accum": TA, "algo": args.algo, "tile": args.tile,
                    "l2": "inputs (%d MiB) %s L2 (126 MB); no flush" % (
                        E * F * T >> 20, "larger than" if E * F * T > 126e6 else "SMALLER than"),
                    "parallelism": "channel shards, %d GPU(s), no collective" % world},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "correlator", "median_launch_ms": kernel_ms,
-                     "nominal_peak": NOMINAL_INT8_TOPS},
+                     "kernel": "tc_pair_kernel (correlator)",
+                     "median_launch_ms": sorted(per_launch)[len(per_launch) // 2],
+                     "nominal_peak": NOMINAL_INT8_TOPS,
+                     "frac_of_nominal": achieved / NOMINAL_INT8_TOPS},
         "pct_of_int8_peak": 100.0 * value / world / peak,
-        "realtime_channels_e2048": value * 1e12 / (E2048_RT_TOPS * 1e12),
-        "gpu_launches": args.steps * launches_per_step(cx, plan),
+        "realtime_channels_e2048_burst": value / E2048_RT_TOPS,
+        "gpu_launches": args.steps,
         "clocks": clocks,
     }
-    if e2e is not None:
-        line["e2e"] = e2e
-    if cpu is not None:
-        line["cpu_baseline"] = cpu
-    if rank == 0:
-        print(json.dumps(line))
+    if clocks_rejected(clocks):
+        line["clocks_rejected"] = True
+    return line, plan, packed, blocks, ops_step
 
 
-def launches_per_step(cx, plan):
-    return 1
+def run_sustained(args, torch, plan, packed, blocks, ops_step, dist, dev, clk, seconds=5.0):
+    """Back-to-back launches of the headline workload for `seconds`, in chunks
+    of launches each timed with CUDA events, with the NVML clock samples of
+    each chunk's window: sustained TOPS, the median SM clock under load and
+    TOPS per MHz (the kernel's speed at the clock it actually ran at)."""
+    stream = torch.cuda.current_stream(dev)
+    # chunk of about 0.2 s of launches
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(10):
+        plan.correlate(packed, blocks, stream=stream)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    per_ms = a.elapsed_time(b) / 10
+    chunk = max(10, int(200.0 / max(per_ms, 1e-3)))
+    nchunks = max(5, int(seconds * 1000.0 / (chunk * per_ms)))
+    if dist is not None:
+        dist.barrier()
+    rows = []
+    t_all0 = time.time()
+    for _ in range(nchunks):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0 = time.time()
+        e0.record(stream)
+        for _ in range(chunk):
+            plan.correlate(packed, blocks, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        h1 = time.time()
+        ms = e0.elapsed_time(e1)
+        win = clk.window(h0, h1)
+        mhz = statistics.median([s[1] for s in win]) if win else None
+        rows.append((ms, mhz))
+    t_all1 = time.time()
+    plan.check_device()
+    total_ms = sum(r[0] for r in rows)
+    total_ms = max_over_ranks(total_ms, dist, dev)
+    launches = chunk * nchunks
+    job_ops = sum_over_ranks(ops_step * launches, dist, dev)
+    tops = job_ops / (total_ms * 1e-3) / 1e12
+    per_chunk = [(ops_step * chunk / (ms * 1e-3) / 1e12, mhz) for ms, mhz in rows]
+    ratios = [t / m for t, m in per_chunk if m]
+    bins = {}
+    for t, m in per_chunk:
+        if m:
+            key = int(round(m / 50.0) * 50)
+            bins.setdefault(key, []).append(t)
+    peak, _ = int8_peak(load_peaks())
+    clocks = clk.summary(t_all0, t_all1)
+    return {
+        "value": tops, "unit": "TOPS", "seconds": total_ms / 1e3, "launches": launches,
+        "chunks": nchunks, "pct_of_int8_peak": 100.0 * tops / (peak * (dist.get_world_size()
+                                                                       if dist else 1)),
+        "sm_mhz_median": clocks.get("sm_mhz"),
+        "tops_per_mhz": statistics.median(ratios) if ratios else None,
+        "tops_by_sm_mhz": {str(k): statistics.median(v) for k, v in sorted(bins.items())},
+        "realtime_channels_e2048": tops / E2048_RT_TOPS,
+        "clocks": clocks,
+        "note": "back-to-back chx_correlate launches of the headline workload; real-time "
+                "channels = sustained TOPS / 6.557 TOPS per E=2048 channel",
+    }
+
+
+def measure_int8_peak(torch, dev, clk, seconds=2.0):
+    """Dense int8 GEMM rate on this GPU in this process: torch._int_mm (cuBLAS)
+    on 8192 x 8192 x 8192 int8 operands resident in HBM, timed with CUDA events
+    over about `seconds`, with the median SM clock of the timed window.  A
+    library GEMM used only as a reference figure for the roofline."""
+    n = 8192
+    g = torch.Generator(device=dev)
+    g.manual_seed(7)
+    a = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev, generator=g)
+    b = torch.randint(-128, 128, (n, n), dtype=torch.int8, device=dev, generator=g)
+    best = None
+    for name, bb in (("B row-major", b), ("B column-major", b.t().contiguous().t())):
+        try:
+            for _ in range(3):
+                torch._int_mm(a, bb)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(5):
+                torch._int_mm(a, bb)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / 5
+            if best is None or ms < best[1]:
+                best = (name, ms, bb)
+        except Exception as e:  # noqa: BLE001
+            err = str(e)
+    if best is None:
+        return {"tops": None, "error": err[:200]}
+    name, ms, bb = best
+    reps = max(10, int(seconds * 1000.0 / ms))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0 = time.time()
+    e0.record()
+    for _ in range(reps):
+        torch._int_mm(a, bb)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    h1 = time.time()
+    ms = e0.elapsed_time(e1) / reps
+    tops = 2.0 * n ** 3 / (ms * 1e-3) / 1e12
+    return {"tops": tops, "ms_per_gemm": ms, "reps": reps, "layout": name,
+            "clocks": clk.summary(h0, h1),
+            "what": "torch._int_mm (cuBLAS int8 GEMM, int32 out), 8192^3, operands in HBM"}
 
 
 def run_e2e(args, torch, cx, plan, dev, ops_step, world, dist):
@@ -414,29 +620,60 @@ def run_e2e(args, torch, cx, plan, dev, ops_step, world, dist):
     d2h.wait_stream(h2d)
     t1.record(d2h)
     torch.cuda.synchronize(dev)
-    ms = t0.elapsed_time(t1)
-    ms = max_over_ranks(ms, dist, dev)
-    return {"value": ops_step * world * steps / (ms * 1e-3) / 1e12, "unit": "TOPS",
+    ms = max_over_ranks(t0.elapsed_time(t1), dist, dev)
+    job_ops = sum_over_ranks(ops_step * steps, dist, dev)
+    return {"value": job_ops / (ms * 1e-3) / 1e12, "unit": "TOPS",
             "h2d_bytes_per_step": nin, "d2h_bytes_per_step": nout * 4,
             "ms_per_step": ms / steps, "steps": steps,
             "pipeline": "2-stage pinned double buffer; H2D, kernel, D2H on three streams"}
 
 
+def cpu_baselines(args):
+    """The reference's CPU correlator on the host cores: all cores on a
+    bounded sample of config 2 (the line's cpu_baseline), plus one core on
+    config 1 in full and on a config-2 sample, with the CPU model."""
+    if args.no_cpu:
+        return None
+    r = cpu_reference_rate(2048, 3072)
+    if r is None:
+        return None
+    out = {"value": r[0] / 1e12, "unit": "TOPS", "cores": r[1], "kind": r[3],
+           "sample": r[2], "seconds": round(r[4], 2), "cpu_model": cpu_model()}
+    single = cpu_single_core()
+    if single is not None:
+        out["single_core"] = single
+    return out
+
+
+def relaunch_under_torchrun(args):
+    """`--gpus N` (N > 1) started as a plain process: run N ranks of this
+    script under torch.distributed.run, one per GPU, and return its status."""
+    port = os.environ.get("MASTER_PORT", "29571")
+    argv = [a for a in sys.argv[1:]]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(args.gpus), "--master-addr", "127.0.0.1",
+           "--master-port", port, os.path.abspath(__file__)] + argv
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--E", type=int, default=2048, help="elements (profiling cases)")
     ap.add_argument("--F", type=int, default=8, help="channels per GPU (profiling cases)")
     ap.add_argument("--T", type=int, default=16384, help="samples (profiling cases)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="plain", choices=["plain", "batched", "stream", "helpers"])
+    ap.add_argument("--config", default="all",
+                    choices=["all", "plain", "batched", "stream", "helpers"])
     ap.add_argument("--algo", default="auto", choices=["auto", "simt", "tc"])
     ap.add_argument("--tsplit", type=int, default=0)
     ap.add_argument("--tile", type=int, default=0, help="tensor-core tile: 0 auto, 1 one SM, 2 SM pair")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sustain-s", type=float, default=5.0,
+                    help="seconds of back-to-back launches for the sustained figure (0: skip)")
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="reference arm: samples per process per step (0: sized so the "
                          "timed steps take ~2.5 min)")
@@ -447,6 +684,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch_under_torchrun(args)
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -454,25 +693,57 @@ def main():
     import chimex as cx
     rank, local_rank, world = env_rank()
     torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
     dist = None
     if world > 1:
         import datetime
         import torch.distributed as tdist
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                 device_id=torch.device("cuda", local_rank))
+                                 device_id=dev)
         dist = tdist
+    import bench_workloads as W
     try:
-        if args.config == "plain":
-            run_plain(args, torch, cx, dist)
-        elif args.config == "batched":
-            import bench_workloads
-            bench_workloads.run_batched(args, torch, cx, dist)
-        elif args.config == "helpers":
-            import bench_workloads
-            bench_workloads.run_helpers(args, torch, cx, dist)
-        else:
-            import bench_workloads
-            bench_workloads.run_stream(args, torch, cx, dist)
+        with ClockSampler(dev) as clk:
+            if args.config in ("all", "plain"):
+                line, plan, packed, blocks, ops_step = run_plain(args, torch, cx, dist, clk)
+                if not args.no_e2e:
+                    line["e2e"] = run_e2e(args, torch, cx, plan, dev, ops_step, world, dist)
+                if args.sustain_s > 0:
+                    sus = run_sustained(args, torch, plan, packed, blocks, ops_step, dist, dev,
+                                        clk, args.sustain_s)
+                    line["sustained"] = sus
+                    line["realtime_channels_e2048"] = sus["realtime_channels_e2048"]
+                del packed, blocks
+                plan.close()
+                torch.cuda.empty_cache()
+                pk = measure_int8_peak(torch, dev, clk)
+                if pk.get("tops"):
+                    pk["kernel_frac_of_this"] = line["roofline"]["achieved"] / pk["tops"]
+                    if "sustained" in line:
+                        pk["sustained_frac_of_this"] = line["sustained"]["value"] / world / pk["tops"]
+                line["int8_peak_in_run"] = pk
+                torch.cuda.empty_cache()
+                if args.config == "all":
+                    line["batched"] = W.run_batched(args, torch, cx, dist, clk)
+                    torch.cuda.empty_cache()
+                    line["stream"] = W.run_stream(args, torch, cx, dist, clk)
+                    torch.cuda.empty_cache()
+                if rank == 0 and world == 1:
+                    cpu = cpu_baselines(args)
+                    if cpu is not None:
+                        line["cpu_baseline"] = cpu
+                if rank == 0:
+                    print(json.dumps(line))
+            elif args.config == "batched":
+                out = W.run_batched(args, torch, cx, dist, clk)
+                if rank == 0:
+                    print(json.dumps(out))
+            elif args.config == "stream":
+                out = W.run_stream(args, torch, cx, dist, clk)
+                if rank == 0:
+                    print(json.dumps(out))
+            else:
+                W.run_helpers(args, torch, cx, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -63,6 +63,7 @@ _sig("chx_blocks_to_triangle", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_blocks_to_full", _i, [_vp, _vp, _vp, _vp])
 _sig("chx_plan_check", _i, [_vp, _vp])
 _sig("chx_correlate_noalloc", _i, [_vp, _vp, _i, _i, _i, _i, _i, _vp])
+_sig("chx_noalloc_check", _i, [_vp])
 _sig("chx_selftest_bounded_wait", _i, [_i, _i, ctypes.POINTER(_i)])
 
 
@@ -104,7 +105,8 @@ EXPORTED = [
     "chx_plan_set_option", "chx_plan_block_words", "chx_plan_input_bytes",
     "chx_plan_sum_words", "chx_plan_triangle_words", "chx_correlate",
     "chx_offset_accumulate", "chx_preseed", "chx_corr_compat", "chx_blocks_to_triangle",
-    "chx_blocks_to_full", "chx_plan_check", "chx_correlate_noalloc", "chx_selftest_bounded_wait",
+    "chx_blocks_to_full", "chx_plan_check", "chx_correlate_noalloc", "chx_noalloc_check",
+    "chx_selftest_bounded_wait",
     "chx_batch_create", "chx_batch_run", "chx_batch_work_units", "chx_batch_ops",
     "chx_batch_check", "chx_batch_destroy", "chx_autotune", "chx_stream_create",
     "chx_stream_admit", "chx_stream_frame_slot", "chx_stream_submit", "chx_stream_last_dump",
@@ -175,6 +177,12 @@ def correlate_noalloc(packed, blocks, E, F, T, upper_triangle_convention=1, accu
                                      upper_triangle_convention, 1 if accumulate else 0,
                                      _stream(stream)))
     return blocks
+
+
+def noalloc_check(stream=None):
+    """chx_noalloc_check: raises ChimexError(E_TIMEOUT) when a bounded device
+    wait of chx_correlate_noalloc gave up since the last check."""
+    check(_lib.chx_noalloc_check(_stream(stream)))
 
 
 class Plan:

@@ -138,6 +138,17 @@ struct Unit {
 static_assert(sizeof(Unit) == 32, "Unit layout");
 
 constexpr int kUnitMaxSamples = 1 << 18;  // int32-exact bound per unit
+constexpr int kUnitStageSamples = 32;      // samples per pipeline stage of both kernels
+
+// Scheduling cost of a unit over samples [t0, t1): its pipeline stages, times
+// the x tiles it converts plus its y tile for the one-SM kernel (nx = 1 or 2
+// x tiles of 128 elements); SM-pair units all convert one y and one x tile per
+// SM, so their cost is their stage count.  Plans, batches, streams and the
+// allocation-free entry point share it so that their schedules agree.
+__host__ __device__ inline int unit_cost(bool pair, int t0, int t1, int nx) {
+    const int stages = (t1 - t0 + kUnitStageSamples - 1) / kUnitStageSamples;
+    return pair ? stages : stages * (2 * nx + 1);
+}
 
 struct TcLaunch {
     const ChanDesc *chans;  // device
@@ -203,6 +214,9 @@ void tc_append_tile_units(int tile, std::vector<Unit> &out, int chan, int E, int
 int tc_tile_slots(int tile, int sm_count);
 cudaError_t tc_tile_launch(int tile, const TcLaunch &L, const CUtensorMap *param_map,
                            const CUtensorMap *param_omap, cudaStream_t st);
+// Device address of the error word of chx_correlate_noalloc on the current
+// device (noalloc.cu); the bounded-wait self-test writes it in mode 2.
+cudaError_t noalloc_error_word(int **out);
 // The autotuner's cached choice for (device, E, T) (batch.cu): true and the
 // tile variant and split count when an entry with the same E and a T within a
 // factor 2 exists.

@@ -15,7 +15,7 @@
 // one SM for an odd one): the integration's samples
 // accumulate in TMEM and each dump buffer is written once, so the resident
 // state never travels through HBM per frame.  An event recorded after each
-// launch is watched by the stream's completion thread, which records, per
+// launch is waited for by the stream's completion thread, which records, per
 // integration, the latency from its last frame's arrival to the moment the
 // completed dump is visible to the host (the compute stream itself never waits
 // on the host).
@@ -130,7 +130,7 @@ struct chx_stream {
 
 namespace {
 
-// Completion thread: waits (spinning on cudaEventQuery) for each launch in
+// Completion thread: waits (blocking, without spinning) for each launch in
 // order and publishes its dumps with their latency.
 void poll_loop(chx_stream *s) {
     cudaSetDevice(s->device);
@@ -140,8 +140,9 @@ void poll_loop(chx_stream *s) {
         if (s->queue.empty()) break;  // stopping with nothing left
         Pending *p = s->queue.front();
         lk.unlock();
-        cudaError_t q;
-        while ((q = cudaEventQuery(p->ev)) == cudaErrorNotReady) std::this_thread::yield();
+        // The event was created with cudaEventBlockingSync: the thread sleeps
+        // until the launch completes instead of occupying a host core.
+        const cudaError_t q = cudaEventSynchronize(p->ev);
         const int64_t t = now_ns();
         lk.lock();
         s->queue.pop_front();
@@ -396,7 +397,8 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     if (!pend) {
         pend = new (std::nothrow) Pending();
         if (!pend) return fail(CHX_E_NOMEM, "host allocation failed");
-        const cudaError_t e = cudaEventCreateWithFlags(&pend->ev, cudaEventDisableTiming);
+        const cudaError_t e =
+            cudaEventCreateWithFlags(&pend->ev, cudaEventDisableTiming | cudaEventBlockingSync);
         if (e != cudaSuccess) {
             delete pend;
             return cuda_fail(e, "completion event");

@@ -54,7 +54,7 @@ namespace {
 
 using namespace tc;
 
-constexpr int kStageSamples = 32;
+constexpr int kStageSamples = kUnitStageSamples;
 constexpr int kOpStages = 4;    // operand ring
 constexpr int kPkStages = 6;    // packed-tile ring
 constexpr int kYOpBytes = 16 * 1024;
@@ -527,7 +527,7 @@ void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t
                 u.t1 = std::min(t_end, u.t0 + chunk);
                 u.out_off = out_off;
                 u.split = splits > 1 ? 1 : 0;
-                u.cost = ((u.t1 - u.t0 + kStageSamples - 1) / kStageSamples) * (2 * nx + 1);
+                u.cost = unit_cost(false, u.t0, u.t1, nx);
                 out.push_back(u);
             }
         }

@@ -44,7 +44,7 @@ namespace {
 
 using namespace tc;
 
-constexpr int kStageSamples = 32;
+constexpr int kStageSamples = kUnitStageSamples;
 constexpr int kOpSlots = 4;     // 2 stage pairs
 constexpr int kPairs = kOpSlots / 2;
 constexpr int kPkStages = 4;
@@ -502,7 +502,7 @@ void tc_append_pair_units(std::vector<Unit> &out, int chan, int E, int t_begin, 
                 u.t1 = std::min(t_end, u.t0 + chunk);
                 u.out_off = out_off;
                 u.split = splits > 1 ? 1 : 0;
-                u.cost = (u.t1 - u.t0 + kStageSamples - 1) / kStageSamples;
+                u.cost = unit_cost(true, u.t0, u.t1, 2);
                 out.push_back(u);
             }
 }

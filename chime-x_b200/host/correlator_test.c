@@ -294,6 +294,7 @@ int main(int argc, char **argv) {
     CU(cudaEventRecord(e1, st));
     CU(cudaEventSynchronize(e1));
     if (!noalloc) CK(chx_plan_check(plan, st));
+    else CK(chx_noalloc_check(st));
     float ms = 0.f;
     CU(cudaEventElapsedTime(&ms, e0, e1));
     const double secs = ms * 1e-3;

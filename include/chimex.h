@@ -157,18 +157,26 @@ int chx_blocks_to_full(chx_plan *plan, const int32_t *d_blocks, int32_t *d_full,
  * This entry point computes exactly what chx_correlate computes for a plan
  * of (E, F, T, upper_triangle_convention), needs no plan and calls no
  * allocator: its work tables live in a fixed-size array inside the library
- * (about 162 KiB on every GPU that loads it, kept until exit).  It uses the
- * plan path's default tile variant and cuts sample ranges only where int32
+ * (about 162 KiB on every GPU that loads it, kept until exit), written on the
+ * device by a small kernel from its launch parameters.  It uses the plan
+ * path's default tile variant and cuts sample ranges only where int32
  * exactness requires it (no automatic split).  Limits: F <= 64 channels and
  * at most 4096 work units (36 per E=2048 channel per 262144 samples); larger
- * calls return CHX_E_UNSUPPORTED.  The first call on each device looks the
- * array up (and so loads the library's device code); make that first call
- * before any stream capture.  All calls share the array: calls whose kernels
- * overlap on the GPU race, so order them on one stream or with events.
- * Device-side wait timeouts are not reported by this entry point. */
+ * calls return CHX_E_UNSUPPORTED.  The first call on each device (and again
+ * after a device reset) looks the array up, which loads the library's device
+ * code; make that first call before any stream capture.  All calls share the
+ * array: calls whose kernels overlap on the GPU race, so order them on one
+ * stream or with events.  Device-side wait timeouts are recorded in the
+ * array and reported by chx_noalloc_check. */
 int chx_correlate_noalloc(const uint8_t *d_packed, int32_t *d_blocks, int num_elements,
                           int num_frequencies, int num_timesamples,
                           int upper_triangle_convention, int accumulate, void *stream);
+
+/* Reads and clears the error word of chx_correlate_noalloc on the current
+ * device: the bounded-wait timeouts of every call made since the last check.
+ * Synchronises the stream; allocates nothing.  Returns CHX_OK or
+ * CHX_E_TIMEOUT.  No counterpart in the reference. */
+int chx_noalloc_check(void *stream);
 
 /* Reads and clears the plan's device error word (bounded-wait timeouts).
  * Synchronises the stream.  Returns CHX_OK or CHX_E_TIMEOUT. */
@@ -178,7 +186,9 @@ int chx_plan_check(chx_plan *plan, void *stream);
  * reference, whose kernels spin without a bound).  Runs one CTA on `device`
  * that waits, with the same helper and 2 s limit as the correlator kernels,
  * on a barrier phase that nothing completes: mode 0 lets the limit run out,
- * mode 1 raises the CTA's abort flag after ~10 ms.  Returns CHX_E_TIMEOUT when
+ * mode 1 raises the CTA's abort flag after ~10 ms, mode 2 does as mode 1 and
+ * then records the give-up in chx_correlate_noalloc's error word (read by
+ * chx_noalloc_check) as a correlator kernel would.  Returns CHX_E_TIMEOUT when
  * the wait gave up as designed (elapsed_ms: how long it waited), CHX_E_INVALID
  * if it claimed completion, CHX_E_CUDA on a CUDA error.  The context stays
  * usable afterwards. */
@@ -284,8 +294,9 @@ int chx_stream_submit(chx_stream *s, int n, const int *channel_ids,
 /* Channel c's last integration whose dump has completed on the device and
  * been published by the stream's completion thread (NULL, seq -1 if none),
  * and its sequence number.  The buffer is overwritten when integration seq+2
- * completes.  Completion is observed by a host thread that polls an event
- * recorded after each launch; chx_stream_sync waits for it. */
+ * completes.  Completion is observed by a host thread that waits (blocking,
+ * without spinning) on an event recorded after each launch; chx_stream_sync
+ * waits for it. */
 int chx_stream_last_dump(chx_stream *s, int channel_id, const int32_t **d_blocks,
                          int64_t *seq);
 /* Counters and latency percentiles over the dumps completed so far. */

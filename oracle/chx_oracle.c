@@ -7,6 +7,7 @@
  */
 #include "chx_oracle.h"
 
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -455,4 +456,108 @@ void orc_visibility(const uint8_t *packed, int T, int F, int E, int f, int y,
     }
     *re = (int32_t)r;
     *im = (int32_t)i;
+}
+
+/* ------------------------------------------------------------------------
+ * Threaded whole-channel correlation for word-for-word checks at full size.
+ * Same visibility definition as accumulate_channel (cpu_corr_test.c:188-193,
+ * Im negated for ut=0 as in cpu_corr_test.c:91-96) and the same block layout
+ * (main_wrapper.c:529-540, preseed_multifreq_UT.cl:128), computed block by
+ * block so that host threads can share the work: each thread takes the next
+ * block from a shared counter and sums its 32 x 32 cells over the samples.
+ */
+struct mt_job {
+    const int16_t *sr, *si; /* channel samples, [t][E], sign-extended */
+    int E, nt, ut;
+    int64_t nb1, nblocks;
+    int64_t next;           /* next block to take (guarded by mu) */
+    pthread_mutex_t mu;
+    int32_t *blocks;
+};
+
+static void *mt_worker(void *arg) {
+    struct mt_job *J = (struct mt_job *)arg;
+    uint32_t acc_re[32][32], acc_im[32][32];
+    const int E = J->E;
+    for (;;) {
+        pthread_mutex_lock(&J->mu);
+        const int64_t b = J->next++;
+        pthread_mutex_unlock(&J->mu);
+        if (b >= J->nblocks) break;
+        /* block b -> (by, bx): walk the rows of the upper triangle */
+        int64_t by = 0, rem = b;
+        while (rem >= J->nb1 - by) {
+            rem -= J->nb1 - by;
+            by++;
+        }
+        const int64_t bx = by + rem;
+        memset(acc_re, 0, sizeof(acc_re));
+        memset(acc_im, 0, sizeof(acc_im));
+        for (int t = 0; t < J->nt; t++) {
+            const int16_t *yr = J->sr + (size_t)t * E + by * 32;
+            const int16_t *yi = J->si + (size_t)t * E + by * 32;
+            const int16_t *xr = J->sr + (size_t)t * E + bx * 32;
+            const int16_t *xi = J->si + (size_t)t * E + bx * 32;
+            for (int yl = 0; yl < 32; yl++) {
+                const int32_t a = yr[yl], c = yi[yl];
+                uint32_t *pr = acc_re[yl], *pi = acc_im[yl];
+                for (int xl = 0; xl < 32; xl++) {
+                    pr[xl] += (uint32_t)(xr[xl] * a + xi[xl] * c);
+                    pi[xl] += (uint32_t)(xr[xl] * c - xi[xl] * a);
+                }
+            }
+        }
+        uint32_t *blk = (uint32_t *)J->blocks + (size_t)b * 2048;
+        for (int yl = 0; yl < 32; yl++)
+            for (int xl = 0; xl < 32; xl++) {
+                blk[(yl * 32 + xl) * 2] = acc_re[yl][xl];
+                blk[(yl * 32 + xl) * 2 + 1] = J->ut ? acc_im[yl][xl] : 0u - acc_im[yl][xl];
+            }
+    }
+    return NULL;
+}
+
+int orc_correlate_channel_mt(const uint8_t *packed, int T, int F, int E, int f,
+                             int t0, int t1, int ut, int nthreads,
+                             int32_t *blocks) {
+    (void)T;
+    if (t1 < t0 || E % 32 != 0 || f < 0 || f >= F) return -1;
+    const int nt = t1 - t0;
+    int16_t *sr = (int16_t *)malloc((size_t)(nt ? nt : 1) * E * sizeof(int16_t));
+    int16_t *si = (int16_t *)malloc((size_t)(nt ? nt : 1) * E * sizeof(int16_t));
+    if (!sr || !si) {
+        free(sr);
+        free(si);
+        return -2;
+    }
+    for (int t = 0; t < nt; t++) {
+        const uint8_t *row = packed + ((size_t)(t0 + t) * F + f) * E;
+        for (int e = 0; e < E; e++) {
+            sr[(size_t)t * E + e] = (int16_t)(((row[e] >> 4) & 0x0F) - 8);
+            si[(size_t)t * E + e] = (int16_t)((row[e] & 0x0F) - 8);
+        }
+    }
+    struct mt_job J;
+    J.sr = sr;
+    J.si = si;
+    J.E = E;
+    J.nt = nt;
+    J.ut = ut;
+    J.nb1 = E / 32;
+    J.nblocks = orc_num_blocks(E);
+    J.next = 0;
+    J.blocks = blocks;
+    pthread_mutex_init(&J.mu, NULL);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    int started = 0;
+    for (int i = 1; i < nthreads; i++)
+        if (pthread_create(&th[started], NULL, mt_worker, &J) == 0) started++;
+    mt_worker(&J); /* the calling thread works too */
+    for (int i = 0; i < started; i++) pthread_join(th[i], NULL);
+    pthread_mutex_destroy(&J.mu);
+    free(sr);
+    free(si);
+    return 0;
 }

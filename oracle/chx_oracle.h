@@ -56,6 +56,13 @@ void orc_correlate_blocks_range(const uint8_t *packed, int T, int F, int E,
                                 int t0, int t1, int ut, int accumulate,
                                 int32_t *blocks);
 
+/* One channel's blocks int32[NB][32][32][2] over samples [t0, t1), the same
+ * values as orc_correlate_blocks_range for channel f, computed block by block
+ * on nthreads host threads (word-for-word checks at full size).  Returns 0. */
+int orc_correlate_channel_mt(const uint8_t *packed, int T, int F, int E, int f,
+                             int t0, int t1, int ut, int nthreads,
+                             int32_t *blocks);
+
 /* Upper-triangle correlation int32[F][E(E+1)/2][2], the reference CPU
  * check (cpu_corr_test.c:156-203 for ut=1, :59-106 for ut=0). */
 void orc_correlate_triangle(const uint8_t *packed, int T, int F, int E, int ut,

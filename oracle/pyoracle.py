@@ -39,6 +39,8 @@ def lib():
         L.orc_correlate_blocks.argtypes = [p, i, i, i, i, i, p]
         L.orc_correlate_blocks_range.argtypes = [p, i, i, i, i, i, i, i, p]
         L.orc_correlate_triangle.argtypes = [p, i, i, i, i, p]
+        L.orc_correlate_channel_mt.restype = i
+        L.orc_correlate_channel_mt.argtypes = [p, i, i, i, i, i, i, i, i, p]
         L.orc_blocks_to_triangle.argtypes = [p, i, i, p]
         L.orc_blocks_to_full.argtypes = [p, i, i, p]
         L.orc_offset_accumulate.argtypes = [p, i, i, i, i, p]
@@ -101,6 +103,19 @@ def correlate_blocks(packed, T, F, E, ut=1, t0=0, t1=None, out=None):
     packed = np.ascontiguousarray(packed, dtype=np.uint8)
     lib().orc_correlate_blocks_range(_ptr(packed), T, F, E, t0,
                                      T if t1 is None else t1, ut, acc, _ptr(out))
+    return out
+
+
+def correlate_channel(packed, T, F, E, f, ut=1, t0=0, t1=None, threads=None):
+    """Channel f's blocks int32[NB*2048] over samples [t0, t1), computed on
+    `threads` host threads (default: every core); the same values as
+    correlate_blocks for that channel."""
+    out = np.empty(num_blocks(E) * 2048, dtype=np.int32)
+    packed = np.ascontiguousarray(packed, dtype=np.uint8)
+    n = threads or os.cpu_count() or 1
+    rc = lib().orc_correlate_channel_mt(_ptr(packed), T, F, E, f, t0,
+                                        T if t1 is None else t1, ut, n, _ptr(out))
+    assert rc == 0, rc
     return out
 
 

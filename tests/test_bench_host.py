@@ -52,3 +52,34 @@ def test_product_package_does_not_reach_the_oracle():
             if "oracle" in text or "pyoracle" in text or "chx_oracle" in text:
                 offenders.append(os.path.relpath(os.path.join(dirpath, f), ROOT))
     assert offenders == []
+
+
+def test_channel_shards_balance_cost():
+    """Largest-first assignment: disjoint shards covering every channel, the
+    same on every rank, with per-rank cost within one channel of the mean."""
+    costs = [5, 1, 9, 3, 3, 7, 2, 8, 4, 6]
+    for world in (1, 2, 3, 4):
+        shards = [bench.shard_channels(costs, world, r) for r in range(world)]
+        flat = sorted(i for sh in shards for i in sh)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in sh) for sh in shards]
+        assert max(loads) - min(loads) <= max(costs)
+    assert bench.shard_channels(costs, 1, 0) == list(range(len(costs)))
+
+
+def test_clock_records_that_reject_a_number():
+    ok = {"sm_mhz": 1950.0, "sm_max_mhz": 1965.0, "reasons": []}
+    assert not bench.clocks_rejected(ok)
+    assert not bench.clocks_rejected(dict(ok, sm_mhz=1400.0, reasons=["sw_power_cap"]))
+    assert bench.clocks_rejected(dict(ok, reasons=["hw_slowdown"]))
+    assert bench.clocks_rejected(dict(ok, reasons=["sw_thermal_slowdown"]))
+    assert bench.clocks_rejected(dict(ok, sm_mhz=900.0))   # stuck low, no reason: a lock
+
+
+def test_default_run_is_bounded():
+    """The driver's default invocation (no flags) runs the headline, sustained,
+    peak, batched and stream legs with a small K and W."""
+    src = open(os.path.join(ROOT, "bench.py")).read()
+    assert 'default="all"' in src
+    assert '"--steps", type=int, default=20' in src
+    assert '"--warmup", type=int, default=5' in src

@@ -1,7 +1,9 @@
 """Multi-process logic of bench.py on CPU (gloo, world size 2): channels are
 independent, so ranks share nothing on the data path; the only cross-rank
 steps are the barrier around the timed region, the max-over-ranks of the
-device times and the sum of per-rank counts, and only rank 0 prints."""
+device times and the sum of per-rank counts, and only rank 0 prints.  The
+batched and streamed channel lists are split between the ranks by
+bench.shard_channels, which every rank computes on its own."""
 import json
 import os
 import socket
@@ -37,8 +39,20 @@ def _rank_main(rank, world, port, out_dir):
         dist.barrier()
         job_ms = bench.max_over_ranks(local_ms, dist, "cpu")
         job_channels = bench.sum_over_ranks(100 + rank, dist, "cpu")  # per-rank counts add up
+        # the config-4 and config-5 channel lists, each rank taking its share
+        import bench_workloads as W
+        Es, TAs = W.config4_channels()
+        costs4 = [bench.vis_ops(E, 4 * T, 1) for E, T in zip(Es, TAs)]
+        mine4 = bench.shard_channels(costs4, w, r)
+        ops4 = bench.sum_over_ranks(sum(costs4[i] for i in mine4), dist, "cpu")
+        E5 = W.config5_channels()
+        costs5 = [bench.vis_ops(E, 1, 1) for E in E5]
+        mine5 = bench.shard_channels(costs5, w, r)
+        ops5 = bench.sum_over_ranks(sum(costs5[i] for i in mine5), dist, "cpu")
         with open(os.path.join(out_dir, "rank%d.json" % rank), "w") as fh:
-            json.dump({"env": [r, lr, w], "job_ms": job_ms, "job_channels": job_channels}, fh)
+            json.dump({"env": [r, lr, w], "job_ms": job_ms, "job_channels": job_channels,
+                       "mine4": mine4, "ops4": ops4, "total4": sum(costs4),
+                       "mine5": mine5, "ops5": ops5, "total5": sum(costs5)}, fh)
     finally:
         dist.destroy_process_group()
 
@@ -48,11 +62,19 @@ def test_max_over_ranks_with_gloo(tmp_path):
     port = free_port()
     mp.start_processes(_rank_main, args=(2, port, str(tmp_path)), nprocs=2, join=True,
                        start_method="spawn")
-    for rank in range(2):
-        rec = json.load(open(tmp_path / ("rank%d.json" % rank)))
+    recs = [json.load(open(tmp_path / ("rank%d.json" % rank))) for rank in range(2)]
+    for rank, rec in enumerate(recs):
         assert rec["env"] == [rank, rank, 2]
         assert rec["job_ms"] == 15.0
         assert rec["job_channels"] == 201.0
+        # the summed per-rank work is the whole list's work
+        assert rec["ops4"] == pytest.approx(rec["total4"])
+        assert rec["ops5"] == pytest.approx(rec["total5"])
+    # the shards are disjoint and cover every channel
+    for key, n in (("mine4", 64), ("mine5", 1024)):
+        a, b = set(recs[0][key]), set(recs[1][key])
+        assert not (a & b) and (a | b) == set(range(n)), key
+        assert abs(len(a) - len(b)) <= n // 4
 
 
 def test_max_over_ranks_without_group():

@@ -166,3 +166,42 @@ def test_full_matrix_view_is_hermitian():
     m = full.reshape(E, E, 2)
     np.testing.assert_array_equal(m[:, :, 0], m[:, :, 0].T)
     np.testing.assert_array_equal(m[:, :, 1], -m[:, :, 1].T)
+
+
+@pytest.mark.parametrize("E,F,T,ut,f", [(32, 1, 1, 1, 0), (96, 3, 37, 1, 2), (256, 2, 100, 0, 1),
+                                         (160, 4, 64, 1, 3)])
+def test_threaded_channel_oracle_equals_restatement(E, F, T, ut, f):
+    """The threaded per-channel oracle used for word-for-word checks at full
+    size gives exactly the single-threaded restatement's blocks, for whole
+    sample ranges and sub-ranges, on one thread and on several."""
+    packed = orc.generate(T, F, E, 4, 31 + E, no_repeat=1)
+    nbw = orc.num_blocks(E) * 2048
+    full = orc.correlate_blocks(packed, T, F, E, ut)[f * nbw:(f + 1) * nbw]
+    for threads in (1, 3):
+        np.testing.assert_array_equal(orc.correlate_channel(packed, T, F, E, f, ut,
+                                                            threads=threads), full)
+    t0, t1 = T // 3, T - T // 4
+    sub = orc.correlate_blocks(packed, T, F, E, ut, t0=t0, t1=t1)[f * nbw:(f + 1) * nbw]
+    np.testing.assert_array_equal(orc.correlate_channel(packed, T, F, E, f, ut, t0=t0, t1=t1), sub)
+
+
+def test_weighted_checks_catch_single_cell_errors():
+    """The full-size checks (four draws of complex nonzero weights) detect an
+    error of one unit in the real part of any single visibility and in the
+    imaginary part of any off-diagonal one, including imaginary-part errors
+    that a real-valued weight product would miss.  (V[y][y] is real by
+    definition and the identity weighs it by |w_y|^2, so its imaginary part
+    is left to the word-for-word and spot checks.)"""
+    import fullsize_checks as fc
+    T, F, E = 24, 1, 64
+    packed = orc.generate(T, F, E, 4, 8, no_repeat=1)
+    good = orc.correlate_blocks(packed, T, F, E, 1)
+    fc.weighted_checks(packed, good, T, F, E, 0, np.random.default_rng(0))
+    rng = np.random.default_rng(1)
+    for trial in range(40):
+        y = int(rng.integers(0, E - 1))
+        x = int(rng.integers(y if trial % 2 == 0 else y + 1, E))
+        bad = good.copy()
+        bad[orc.block_cell_offset(E, 0, y, x) + (trial % 2)] += 1
+        with pytest.raises(AssertionError):
+            fc.weighted_checks(packed, bad, T, F, E, 0, np.random.default_rng(trial))

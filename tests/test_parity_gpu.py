@@ -1,9 +1,12 @@
 """GPU parity of libchimex against the CPU oracle, through the C ABI.
 
 Bit-exact integer comparisons: every output word must equal the oracle's.
-Small and golden cases compare whole buffers; the full BASELINE sizes use
-size-independent properties (weighted checksums over every element, exact
-constant-input values, random spot checks against O(T) direct sums).
+Small and golden cases compare whole buffers.  At the full BASELINE sizes one
+channel per configuration is compared word for word with the oracle run on
+all host cores, and every channel is checked by size-independent properties:
+weighted checksums over every visibility (complex nonzero weights, four
+draws), exact constant-input values and spot visibilities against O(T)
+direct sums.
 """
 import json
 import os
@@ -11,6 +14,7 @@ import os
 import numpy as np
 import pytest
 
+import fullsize_checks as fc
 import pyoracle as orc
 
 torch = pytest.importorskip("torch")
@@ -201,42 +205,111 @@ def test_reorg_kernels(chimex):
                                   orc.blocks_to_full(ref_blocks, F, E))
 
 
-def _checksums(packed, blocks, T, F, E, seed, nspot=64):
-    rng = np.random.default_rng(seed)
-    for f in range(F):
-        w = rng.integers(-3, 4, size=2 * E).astype(np.int32)
-        assert orc.weighted_power(packed, T, F, E, f, w) == \
-            orc.weighted_from_blocks(blocks, F, E, f, w), "checksum of channel %d" % f
-        for _ in range(nspot):
-            y = int(rng.integers(0, E))
-            x = int(rng.integers(32 * (y // 32), E))
-            off = orc.block_cell_offset(E, f, y, x)
-            assert orc.visibility(packed, T, F, E, f, y, x) == \
-                (blocks[off], blocks[off + 1]), (f, y, x)
+# ------------------------------------------------------------------ full sizes
+# Configs 2 and 3 at their own sizes.  One channel of each is compared word for
+# word (every cell of every block, diagonal-block lower halves included) with
+# the oracle computed on all host cores; every channel is checked by four
+# weighted checksums with complex nonzero weights and by spot visibilities.
+
+_FULL = {}
+
+
+def _config2():
+    """E=2048, F=8, T=16384, reference generator (random, seed 42, no repeat)."""
+    if "c2" not in _FULL:
+        E, F, T = 2048, 8, 16384
+        packed = orc.generate(T, F, E, 4, 42, no_repeat=1)
+        f = 5
+        _FULL["c2"] = (E, F, T, packed, f, orc.correlate_channel(packed, T, F, E, f, 1))
+    return _FULL["c2"]
+
+
+def _config3():
+    """E=2048, F=16, time_accum=1912, T=1912*8; channels 0-7 constant -8 (the
+    int32 worst case |Re| = 128 T), channels 8-15 random (seed 42, no repeat)."""
+    if "c3" not in _FULL:
+        E, F, T = 2048, 16, 1912 * 8
+        const = orc.generate(T, 8, E, 1, 42, initial_re=-8, initial_im=-8)
+        rnd = orc.generate(T, 8, E, 4, 42, no_repeat=1)
+        packed = np.concatenate([const.reshape(T, 8, E), rnd.reshape(T, 8, E)], axis=1).ravel()
+        f = 12
+        _FULL["c3"] = (E, F, T, packed, f, orc.correlate_channel(packed, T, F, E, f, 1))
+    return _FULL["c3"]
+
+
+def _config3_single_channel():
+    """Config 3 with generate_frequency = 5: channel 5 random (seed 42, no
+    repeat), every other channel the default value re = 7, im = -8
+    (input_generator.c:84-96)."""
+    if "c3q" not in _FULL:
+        E, F, T, q = 2048, 16, 1912 * 8, 5
+        packed = orc.generate(T, F, E, 4, 42, 7, -8, 0, 0, q, 1)
+        _FULL["c3q"] = (E, F, T, packed, q, orc.correlate_channel(packed, T, F, E, q, 1))
+    return _FULL["c3q"]
 
 
 @pytest.mark.parametrize("algo", ALGOS)
 def test_full_size_plain_config(chimex, algo):
     """E=2048, F=8, T=16384, random no-repeat."""
-    E, F, T = 2048, 8, 16384
-    packed = orc.generate(T, F, E, 4, 42, no_repeat=1)
+    E, F, T, packed, f, ref = _config2()
     blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
-    _checksums(packed, blocks, T, F, E, seed=1)
+    np.testing.assert_array_equal(fc.channel_blocks(blocks, E, f), ref)
+    rng = np.random.default_rng(1)
+    for g in range(F):
+        fc.weighted_checks(packed, blocks, T, F, E, g, rng)
+        fc.spot_checks(packed, blocks, T, F, E, g, rng, 16)
 
 
 @pytest.mark.parametrize("algo", ALGOS)
 def test_full_size_overflow_edge_config(chimex, algo):
-    """E=2048, F=16, T=1912*8; channels 0-7 constant -8
-    (|Re| = 128 T, the int32 worst case), channels 8-15 seeded random."""
-    E, F, T = 2048, 16, 1912 * 8
-    const = orc.generate(T, 8, E, 1, 42, initial_re=-8, initial_im=-8)
-    rnd = orc.generate(T, 8, E, 4, 42, no_repeat=1)
-    packed = np.concatenate([const.reshape(T, 8, E), rnd.reshape(T, 8, E)], axis=1).ravel()
+    """BASELINE config 3: constant -8 channels reach |Re| = 128 T exactly;
+    the random channels are checked word for word (one) and by checksums."""
+    E, F, T, packed, f, ref = _config3()
     blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
     nbw = orc.num_blocks(E) * 2048
     head = blocks[: 8 * nbw]
     assert (head[0::2] == 128 * T).all() and (head[1::2] == 0).all()
-    _checksums(packed, blocks, T, F, E, seed=2, nspot=16)
+    np.testing.assert_array_equal(fc.channel_blocks(blocks, E, f), ref)
+    rng = np.random.default_rng(2)
+    for g in range(8, F):
+        fc.weighted_checks(packed, blocks, T, F, E, g, rng)
+        fc.spot_checks(packed, blocks, T, F, E, g, rng, 8)
+
+
+@pytest.mark.parametrize("algo", ALGOS)
+def test_full_size_single_channel_generator(chimex, algo):
+    """Config 3 with generate_frequency: the fixed channels hold exactly
+    T * |7 - 8i|^2 = 113 T (imaginary 0) in every cell, the generated channel
+    equals the oracle word for word."""
+    E, F, T, packed, q, ref = _config3_single_channel()
+    blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
+    for g in range(F):
+        ch = fc.channel_blocks(blocks, E, g)
+        if g == q:
+            np.testing.assert_array_equal(ch, ref)
+        else:
+            assert (ch[0::2] == 113 * T).all() and (ch[1::2] == 0).all(), g
+
+
+@pytest.mark.parametrize("kb", [0, 1])
+@pytest.mark.parametrize("ut", [0, 1])
+def test_full_size_offset_sums_and_preseed(chimex, kb, ut):
+    """The standalone offset_accumulator and all four preseed variants at
+    config 3's size (E=2048, F=16, T=15296), word for word against the
+    oracle's restatement of offset_accumulator.cl:18-47 and
+    preseed_multifreq*_UT.cl / preseed_multifreq*.cl."""
+    E, F, T, packed, _, _ = _config3()
+    p = chimex.Plan(E, F, T, 1912, ut, kb, 0)
+    d = to_dev(packed)
+    sums = p.offset_accumulate(d)
+    ref_sums = _FULL.get("c3sums")
+    if ref_sums is None:
+        ref_sums = _FULL["c3sums"] = orc.offset_accumulate(packed, T, F, E)
+    np.testing.assert_array_equal(sums.cpu().numpy().view(np.uint32), ref_sums)
+    blocks = p.preseed(sums)
+    np.testing.assert_array_equal(blocks.cpu().numpy(), orc.preseed(ref_sums, T, F, E, kb, ut))
+    p.check_device()
+    p.close()
 
 
 @pytest.mark.parametrize("E,F,T", [(2048, 16, 4096), (1024, 16, 15296), (2048, 32, 2048),

@@ -65,6 +65,46 @@ def test_stream_dumps_match_oracle(chimex):
 
 
 @pytest.mark.gpu
+def test_stream_config5_shape_dumps_match_oracle(chimex):
+    """Config 5's channel shape: E=2048 and E=1024 channels, time_accum 1024,
+    frames of 256 samples, three integrations per channel with staggered
+    starts (so completions of different channels fall on different ticks and
+    on the same tick); every dump is compared word for word with the oracle
+    for exactly its integration's frames."""
+    cx = chimex
+    frame, ta, nint = 256, 1024, 3
+    layout = [2048, 1024, 2048, 1024, 2048]
+    s = cx.Stream(len(layout), frame)
+    ids = [s.admit(E, ta) for E in layout]
+    per = ta // frame
+    start = {c: (c * 3) % per for c in ids}   # first tick of channel c
+    rng = np.random.default_rng(55)
+    history = {c: [] for c in ids}
+    checked = 0
+    for tick in range(per * nint + per):
+        sub = [c for c in ids if tick >= start[c] and len(history[c]) < per * nint]
+        if not sub:
+            continue
+        host = [rng.integers(0, 256, size=(frame, layout[c]), dtype=np.uint8) for c in sub]
+        s.submit(sub, [torch.from_numpy(h.reshape(-1)).cuda() for h in host])
+        s.sync()
+        for c, h in zip(sub, host):
+            history[c].append(h)
+            if len(history[c]) % per == 0:
+                seq = len(history[c]) // per - 1
+                got, got_seq = dump_of(s, c)
+                assert got_seq == seq
+                x = np.concatenate(history[c][seq * per:(seq + 1) * per]).reshape(-1)
+                ref = orc.correlate_channel(x, ta, 1, layout[c], 0, 1)
+                np.testing.assert_array_equal(got, ref, err_msg="channel %d dump %d" % (c, seq))
+                checked += 1
+    s.check_device()
+    assert checked == len(layout) * nint
+    assert s.stats()["dumps"] == checked
+    s.close()
+
+
+@pytest.mark.gpu
 def test_stream_in_place_frames_reuse_ring(chimex):
     """Frames submitted in place (no copy) correlate what the ring holds: two
     integrations after a copied integration, the same ring half gives the
