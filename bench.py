@@ -674,6 +674,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sustain-s", type=float, default=5.0,
                     help="seconds of back-to-back launches for the sustained figure (0: skip)")
+    ap.add_argument("--no-peak", action="store_true",
+                    help="skip the in-run int8 GEMM reference (profiling runs)")
     ap.add_argument("--ref-sample", type=int, default=0,
                     help="reference arm: samples per process per step (0: sized so the "
                          "timed steps take ~2.5 min)")
@@ -716,7 +718,7 @@ def main():
                 del packed, blocks
                 plan.close()
                 torch.cuda.empty_cache()
-                pk = measure_int8_peak(torch, dev, clk)
+                pk = {"skipped": True} if args.no_peak else measure_int8_peak(torch, dev, clk)
                 if pk.get("tops"):
                     pk["kernel_frac_of_this"] = line["roofline"]["achieved"] / pk["tops"]
                     if "sustained" in line:

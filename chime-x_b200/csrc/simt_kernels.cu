@@ -268,41 +268,72 @@ __device__ __forceinline__ void preseed_block(const uint32_t *sx, const uint32_t
     }
 }
 
-// One CTA per block: 16.6k CTAs at E = 2048, F = 8 keep enough stores in
-// flight (a CTA per run of blocks, with the channel's sums in shared memory,
-// measured 1.8x slower).
+// One CTA per run of kPsBlocks consecutive blocks of one channel: every
+// thread issues its 2 x kPsBlocks 16-byte stores back to back (no dependency
+// between them), which keeps more bytes in flight per thread than one block
+// per CTA.  The blocks' row and column sums are gathered into shared memory
+// first.
+constexpr int kPsBlocks = 4;
+
 __global__ void __launch_bounds__(256)
 preseed_kernel(const uint32_t *__restrict__ sums, int32_t *__restrict__ blocks, int E,
                int nb1, int64_t nb, uint32_t t128, int packed_variant, int ut) {
-    __shared__ uint32_t sx[64], sy[64];
-    const int b = blockIdx.x, f = blockIdx.y;
-    int by, bx;
-    decode_block(b, nb1, by, bx);
+    __shared__ uint32_t sx[kPsBlocks][64], sy[kPsBlocks][64];
+    const int f = blockIdx.y;
+    const int64_t b0 = (int64_t)blockIdx.x * kPsBlocks;
     const int tid = threadIdx.x;
-    if (tid < 64) {
-        sx[tid] = sums[((int64_t)f * E + bx * 32) * 2 + tid];
-        sy[tid] = sums[((int64_t)f * E + by * 32) * 2 + tid];
+    for (int i = tid; i < kPsBlocks * 64; i += 256) {
+        const int k = i >> 6, w = i & 63;
+        if (b0 + k < nb) {
+            int by, bx;
+            decode_block((int)(b0 + k), nb1, by, bx);
+            sx[k][w] = sums[((int64_t)f * E + bx * 32) * 2 + w];
+            sy[k][w] = sums[((int64_t)f * E + by * 32) * 2 + w];
+        }
     }
     __syncthreads();
-    preseed_block(sx, sy, blocks + ((int64_t)f * nb + b) * 2048, t128, packed_variant, ut, tid);
+#pragma unroll
+    for (int k = 0; k < kPsBlocks; k++)
+        if (b0 + k < nb)
+            preseed_block(sx[k], sy[k], blocks + ((int64_t)f * nb + b0 + k) * 2048, t128,
+                          packed_variant, ut, tid);
 }
 
-// Block layout -> packed triangle (gpu_data_reorg.c:76-124).
+// Block layout -> packed triangle (gpu_data_reorg.c:76-124).  The block is
+// read into shared memory with 16-byte loads; each of its rows is a
+// contiguous run of cells in the triangle (x >= y only on the diagonal
+// block) starting at any cell index, so every row is written as 16-byte
+// stores of cell pairs, with a single 8-byte store for an odd first cell and
+// for an odd last cell.  16 threads per row, two rows per thread.
 __global__ void __launch_bounds__(256)
 blocks_to_triangle_kernel(const int32_t *__restrict__ blocks, int32_t *__restrict__ tri,
                           int E, int nb1, int64_t nb) {
+    __shared__ __align__(16) int2 cells[32 * 32];
     const int b = blockIdx.x, f = blockIdx.y;
     int by, bx;
     decode_block(b, nb1, by, bx);
     const int64_t ntri = (int64_t)E * (E + 1) / 2;
-    const int32_t *blk = blocks + ((int64_t)f * nb + b) * 2048;
+    const int4 *blk = reinterpret_cast<const int4 *>(blocks + ((int64_t)f * nb + b) * 2048);
+    int4 *c4 = reinterpret_cast<int4 *>(cells);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int c = threadIdx.x + 256 * k, yl = c >> 5, xl = c & 31;
-        if (bx == by && xl < yl) continue;
-        const int64_t y = by * 32 + yl, x = bx * 32 + xl;
-        const int64_t a = f * ntri + y * E - (y - 1) * y / 2 + (x - y);
-        *reinterpret_cast<int2 *>(tri + 2 * a) = *reinterpret_cast<const int2 *>(blk + 2 * c);
+    for (int k = 0; k < 2; k++) c4[threadIdx.x + 256 * k] = __ldg(blk + threadIdx.x + 256 * k);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int slot = threadIdx.x + 256 * r, yl = slot >> 4, k = slot & 15;
+        const int xs = (bx == by) ? yl : 0;  // first cell of the row written
+        const int64_t y = by * 32 + yl;
+        const int64_t a0 = f * ntri + y * E - (y - 1) * y / 2 + (bx * 32 + xs - y);
+        const int head = (int)(a0 & 1);      // odd start: one 8-byte cell first
+        const int n = 32 - xs - head;        // cells after the head
+        const int2 *row = cells + yl * 32;
+        if (k < n / 2) {
+            const int x = xs + head + 2 * k;
+            const int2 u = row[x], v = row[x + 1];
+            *reinterpret_cast<int4 *>(tri + 2 * (a0 + head + 2 * k)) = make_int4(u.x, u.y, v.x, v.y);
+        }
+        if (k == 15 && head) *reinterpret_cast<int2 *>(tri + 2 * a0) = row[xs];
+        if (k == 14 && (n & 1)) *reinterpret_cast<int2 *>(tri + 2 * (a0 + 31 - xs)) = row[31];
     }
 }
 
@@ -383,7 +414,7 @@ cudaError_t launch_offset_accumulate(const uint8_t *packed, uint32_t *sums, int 
 cudaError_t launch_preseed(const uint32_t *sums, int32_t *blocks, int E, int F, int T,
                            int packed_variant, int ut, cudaStream_t st) {
     const int64_t nb = num_blocks_of(E);
-    dim3 grid((unsigned)nb, (unsigned)F);
+    dim3 grid((unsigned)((nb + kPsBlocks - 1) / kPsBlocks), (unsigned)F);
     preseed_kernel<<<grid, 256, 0, st>>>(sums, blocks, E, E / 32, nb, (uint32_t)T * 128u,
                                          packed_variant, ut);
     return cudaGetLastError();
