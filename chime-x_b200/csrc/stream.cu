@@ -130,8 +130,8 @@ struct chx_stream {
 
 namespace {
 
-// Completion thread: waits (blocking, without spinning) for each launch in
-// order and publishes its dumps with their latency.
+// Completion thread: waits (polling with short sleeps, not spinning) for each
+// launch in order and publishes its dumps with their latency.
 void poll_loop(chx_stream *s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
@@ -140,9 +140,16 @@ void poll_loop(chx_stream *s) {
         if (s->queue.empty()) break;  // stopping with nothing left
         Pending *p = s->queue.front();
         lk.unlock();
-        // The event was created with cudaEventBlockingSync: the thread sleeps
-        // until the launch completes instead of occupying a host core.
-        const cudaError_t q = cudaEventSynchronize(p->ev);
+        // Poll the event with 20 us sleeps in between: the thread takes a few
+        // percent of a host core instead of spinning on one, and sees the
+        // completion within ~20-70 us.  (A blocking-sync event waited on with
+        // cudaEventSynchronize measured 0.96 ms p50 frame-to-dump latency on
+        // B200, against 0.65 ms for polling: the wake-up comes late.)
+        cudaError_t q;
+        while ((q = cudaEventQuery(p->ev)) == cudaErrorNotReady) {
+            timespec ts{0, 20000};
+            nanosleep(&ts, nullptr);
+        }
         const int64_t t = now_ns();
         lk.lock();
         s->queue.pop_front();
@@ -397,8 +404,7 @@ int chx_stream_submit(chx_stream *s, int n, const int *ids, const uint8_t *const
     if (!pend) {
         pend = new (std::nothrow) Pending();
         if (!pend) return fail(CHX_E_NOMEM, "host allocation failed");
-        const cudaError_t e =
-            cudaEventCreateWithFlags(&pend->ev, cudaEventDisableTiming | cudaEventBlockingSync);
+        const cudaError_t e = cudaEventCreateWithFlags(&pend->ev, cudaEventDisableTiming);
         if (e != cudaSuccess) {
             delete pend;
             return cuda_fail(e, "completion event");

@@ -294,9 +294,9 @@ int chx_stream_submit(chx_stream *s, int n, const int *channel_ids,
 /* Channel c's last integration whose dump has completed on the device and
  * been published by the stream's completion thread (NULL, seq -1 if none),
  * and its sequence number.  The buffer is overwritten when integration seq+2
- * completes.  Completion is observed by a host thread that waits (blocking,
- * without spinning) on an event recorded after each launch; chx_stream_sync
- * waits for it. */
+ * completes.  Completion is observed by a host thread that polls, with
+ * 20 us sleeps in between, an event recorded after each launch;
+ * chx_stream_sync waits for it. */
 int chx_stream_last_dump(chx_stream *s, int channel_id, const int32_t **d_blocks,
                          int64_t *seq);
 /* Counters and latency percentiles over the dumps completed so far. */
