@@ -537,12 +537,10 @@ void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t
 void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets) {
     // Longest-processing-time-first: hand each unit, largest first, to the
     // CTA with the least assigned cost, then store the units CTA by CTA.
-    // Within a CTA the units run in (channel, sample range, tile) order: a
-    // CTA's total, and so the makespan, does not depend on that order, and it
-    // makes the CTAs step through the channels together, so that the tiles
-    // one channel's units share are read from L2 rather than again from DRAM
-    // (in cost order, the cheaper units of every channel would all run at
-    // the end and re-read every channel's samples).
+    // Each CTA keeps the largest-first order: equal-cost units of one channel
+    // and sample range then sit on neighbouring CTAs at the same time and
+    // share its tiles in L2.  (Ordering each CTA's units by channel instead
+    // measured 2.5x the input in DRAM reads at E=1920, against 1.97x.)
     std::stable_sort(u.begin(), u.end(),
                      [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
     if (grid < 1) grid = 1;
@@ -568,13 +566,6 @@ void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets) {
     std::vector<int> fill(offsets.begin(), offsets.end() - 1);
     std::vector<Unit> out(u.size());
     for (size_t i = 0; i < u.size(); i++) out[fill[owner[i]]++] = u[i];
-    for (int b = 0; b < grid; b++)
-        std::stable_sort(out.begin() + offsets[b], out.begin() + offsets[b + 1],
-                         [](const Unit &a, const Unit &c) {
-                             if (a.chan != c.chan) return a.chan < c.chan;
-                             if (a.t0 != c.t0) return a.t0 < c.t0;
-                             return a.tyx < c.tyx;
-                         });
     u.swap(out);
 }
 
