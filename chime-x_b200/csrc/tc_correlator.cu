@@ -535,14 +535,16 @@ void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t
 }
 
 void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets) {
-    // Longest-processing-time-first: hand each unit, largest first, to the
-    // CTA with the least assigned cost, then store the units CTA by CTA.
-    // Each CTA keeps the largest-first order: equal-cost units of one channel
-    // and sample range then sit on neighbouring CTAs at the same time and
-    // share its tiles in L2.  (Ordering each CTA's units by channel instead
-    // measured 2.5x the input in DRAM reads at E=1920, against 1.97x.)
+    // Longest-processing-time-first: hand each unit, longest sample range
+    // first, to the CTA with the least assigned cost, then store the units
+    // CTA by CTA.  Units of equal range keep their enumeration order (channel
+    // by channel, tile by tile), so the units of one channel and sample range
+    // sit on neighbouring CTAs at the same time and share its tiles in L2.
+    // Sorting by full cost instead would move the one-SM kernel's cheaper
+    // one-x-tile units of every channel to the end, where they re-read every
+    // channel's samples from DRAM (E=1920: 2.4x the input read).
     std::stable_sort(u.begin(), u.end(),
-                     [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
+                     [](const Unit &a, const Unit &b) { return a.t1 - a.t0 > b.t1 - b.t0; });
     if (grid < 1) grid = 1;
     std::vector<long long> load(grid, 0);
     std::vector<int> owner(u.size());
