@@ -535,16 +535,16 @@ void tc_append_units(std::vector<Unit> &out, int chan, int E, int t_begin, int t
 }
 
 void tc_schedule(std::vector<Unit> &u, int grid, std::vector<int> &offsets) {
-    // Longest-processing-time-first: hand each unit, longest sample range
-    // first, to the CTA with the least assigned cost, then store the units
-    // CTA by CTA.  Units of equal range keep their enumeration order (channel
-    // by channel, tile by tile), so the units of one channel and sample range
-    // sit on neighbouring CTAs at the same time and share its tiles in L2.
-    // Sorting by full cost instead would move the one-SM kernel's cheaper
-    // one-x-tile units of every channel to the end, where they re-read every
-    // channel's samples from DRAM (E=1920: 2.4x the input read).
+    // Longest-processing-time-first: hand each unit, largest first, to the
+    // CTA with the least assigned cost, then store the units CTA by CTA.  For
+    // the one-SM kernel this puts every channel's cheaper one-x-tile units at
+    // the end, where they read the channels' samples from DRAM a second time
+    // (E=1920, F=8: 2.4x the input).  Orders that keep a channel's units
+    // together read less (1.65x by sample range, then enumeration order) but
+    // balance the CTAs worse and measured slower (1825 vs 2033 TOPS), and
+    // ordering each CTA's units by channel read more (2.5x).
     std::stable_sort(u.begin(), u.end(),
-                     [](const Unit &a, const Unit &b) { return a.t1 - a.t0 > b.t1 - b.t0; });
+                     [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
     if (grid < 1) grid = 1;
     std::vector<long long> load(grid, 0);
     std::vector<int> owner(u.size());
