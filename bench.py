@@ -12,9 +12,9 @@ The default run prints ONE JSON line holding, besides the headline value:
                     the SM clock sampled, binned by clock; real-time channels
   int8_peak_in_run  a cuBLAS int8 GEMM (torch._int_mm, 8192^3) timed in the
                     same process, with its median SM clock
-  batched           BASELINE config 4: 64 ragged channels in one CUDA-graph
+  batched           the 64-channel ragged batch in one CUDA-graph
                     launch against the plain per-channel launches
-  stream            BASELINE config 5: 1024-channel streaming loop, real-time
+  stream            the 1024-channel streaming loop, real-time
                     channels sustained, p50/p99 frame-to-visibility latency
   e2e, cpu_baseline, roofline, clocks, gpu_launches
 
@@ -293,9 +293,10 @@ def cpu_reference_rate(E, T_sample, max_procs=None, no_repeat=1, seed0=42):
 
 
 def cpu_single_core():
-    """The reference CPU correlator on ONE core: BASELINE config 1 in full
+    """The reference CPU correlator on ONE core: the small plain case in full
     (E=256, F=1, T=256, seed 42, repeating generator), repeated for about a
-    second, and a bounded sample of config 2 (E=2048, F=1, T=512, no repeat).
+    second, and a bounded sample of the full-size plain workload (E=2048, F=1, T=512,
+    no repeat).
     Each figure is the reference's own timing of its correlation loop."""
     driver = _ref_driver()
     if driver is None:
@@ -313,12 +314,12 @@ def cpu_single_core():
     secs = statistics.median(r["seconds"] for r in recs)
     out["config1"] = {"value": OPS_PER_VIS_SAMPLE * recs[0]["updates"] / secs / 1e12,
                       "unit": "TOPS", "seconds": secs, "runs": len(recs),
-                      "sample": "E=256 F=1 T=256 seed 42 repeat (config 1 in full)",
+                      "sample": "E=256 F=1 T=256 seed 42 repeat (the small plain case in full)",
                       "triangle_fnv": recs[0]["hash"]}
     r2 = run(512, 2048, 1)
     out["config2_sample"] = {"value": OPS_PER_VIS_SAMPLE * r2["updates"] / r2["seconds"] / 1e12,
                              "unit": "TOPS", "seconds": r2["seconds"],
-                             "sample": "E=2048 F=1 T=512 seed 42 no repeat (1/256 of config 2)"}
+                             "sample": "E=2048 F=1 T=512 seed 42 no repeat (1/256 of the full-size plain workload)"}
     return out
 
 
@@ -380,7 +381,7 @@ def make_plain_plan(args, cx, local_rank):
 
 
 def run_plain(args, torch, cx, dist, clk):
-    """The headline leg: one chx_correlate launch of config 2 per step."""
+    """The headline leg: one chx_correlate launch of E=2048 F=8 T=16384 per step."""
     rank, local_rank, world = env_rank()
     E, F, T, TA = args.E, args.F, args.T, 256
     dev = torch.device("cuda", local_rank)
@@ -630,8 +631,9 @@ def run_e2e(args, torch, cx, plan, dev, ops_step, world, dist):
 
 def cpu_baselines(args):
     """The reference's CPU correlator on the host cores: all cores on a
-    bounded sample of config 2 (the line's cpu_baseline), plus one core on
-    config 1 in full and on a config-2 sample, with the CPU model."""
+    bounded sample of the full-size plain workload (the line's cpu_baseline),
+    plus one core on the small plain case (E=256, T=256) in full and on a
+    sample of the full-size workload, with the CPU model."""
     if args.no_cpu:
         return None
     r = cpu_reference_rate(2048, 3072)

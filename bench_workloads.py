@@ -1,13 +1,13 @@
 """Batched and streaming legs of bench.py (sub-objects of the default line,
 or one line each with --config batched|stream).
 
-batched (BASELINE config 4): 64 channels with element counts drawn from
+batched: 64 channels with element counts drawn from
 {256, 512, 1024, 1536, 2048} and time_accum uniform in [64, 1912] (seed 42),
 4 integrations each, all in one persistent launch replayed from a CUDA graph
 (chx_batch_run), against the plain per-channel path: one chx_correlate
 launch per channel and integration.
 
-stream (BASELINE config 5): 1024 channels (70% E=2048, 30% E=1024, seed 42),
+stream: 1024 channels (70% E=2048, 30% E=1024, seed 42),
 frames of 256 samples, time_accum 1024, admitted by free HBM.  Channels start
 a quarter integration apart so that a quarter of them complete per frame
 tick.  Phases: flat out (ticks back to back: sustained real-time channels);
@@ -46,7 +46,7 @@ def _peak():
 
 
 def config4_channels():
-    """(E, time_accum) of BASELINE config 4's 64 channels (seed 42)."""
+    """(E, time_accum) of the ragged batch's 64 channels (seed 42)."""
     import numpy as np
     rng = np.random.default_rng(42)
     Es = [int(e) for e in rng.choice([256, 512, 1024, 1536, 2048], size=64)]
@@ -55,7 +55,7 @@ def config4_channels():
 
 
 def config5_channels():
-    """Element counts of BASELINE config 5's 1024 channels: 717 with E=2048,
+    """Element counts of the streaming workload's 1024 channels: 717 with E=2048,
     307 with E=1024, order shuffled with seed 42."""
     import numpy as np
     Es = [2048] * 717 + [1024] * 307
@@ -147,7 +147,7 @@ def run_batched(args, torch, cx, dist, clk):
     value = job_ops / (ms_batch * 1e-3) / 1e12
     peak, peak_src = _peak()
     out = {
-        "metric": "exact INT8-TC TOPS (batched ragged, BASELINE config 4)", "value": value,
+        "metric": "exact INT8-TC TOPS (batched ragged, 64 channels)", "value": value,
         "unit": "TOPS", "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": ms_batch, "higher_is_better": True,
         "scaling": "strong" if world > 1 else "n/a (one GPU)",
@@ -416,7 +416,7 @@ def run_stream(args, torch, cx, dist, clk):
     peak, peak_src = _peak()
     stream_ms_tick = ms / ticks
     out = {
-        "metric": "real-time channels sustained (stream, BASELINE config 5)",
+        "metric": "real-time channels sustained (stream, 1024 channels)",
         "value": rt_channels, "unit": "channels", "n_gpus": world, "steps": ticks, "warmup": warm,
         "ms_per_step": stream_ms_tick, "higher_is_better": True,
         "scaling": "strong" if world > 1 else "n/a (one GPU)",

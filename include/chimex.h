@@ -43,7 +43,7 @@ extern "C" {
 
 #define CHX_OK 0
 #define CHX_E_INVALID (-1)     /* bad argument or shape */
-#define CHX_E_UNSUPPORTED (-2) /* valid, but outside what this build handles */
+#define CHX_E_UNSUPPORTED (-2) /* valid, but outside what this library handles */
 #define CHX_E_CUDA (-3)        /* a CUDA runtime call failed */
 #define CHX_E_NOMEM (-4)       /* device or host allocation failed */
 #define CHX_E_TIMEOUT (-5)     /* a bounded device-side wait gave up */

@@ -45,7 +45,7 @@ def fnv1a_bytes(b):
 
 # (T, F, E, gen, seed, dre, dim, ire, iim, single_freq, no_repeat, ut)
 CASES = [
-    # E=256 F=1 T=TA=256, seed 42, repeating random.
+    # The small plain case: E=256 F=1 T=TA=256, seed 42, repeating random.
     (256, 1, 256, 4, 42, 0, 0, 0, 0, -1, 0, 1),
     (256, 1, 256, 4, 42, 0, 0, 0, 0, -1, 1, 1),
     (256, 1, 256, 1, 42, 0, 0, 0, 0, -1, 0, 1),
@@ -59,7 +59,7 @@ CASES = [
     (64, 4, 128, 2, 42, 0, 0, 0, 0, -1, 0, 1),
     (64, 4, 128, 3, 42, 0, 0, 0, 0, -1, 0, 1),
     (64, 4, 128, 2, 42, 0, 0, 3, -5, -1, 0, 0),
-    # single-channel override (config 3 style: default (7, -8) elsewhere)
+    # single-channel override (default (7, -8) in every other channel)
     (64, 4, 128, 4, 42, 7, -8, 0, 0, 2, 1, 1),
     (64, 4, 128, 4, 42, 7, -8, 0, 0, 4, 1, 1),  # == F: every channel default
     # small shapes kept whole in small_tri.npz

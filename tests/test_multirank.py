@@ -39,7 +39,7 @@ def _rank_main(rank, world, port, out_dir):
         dist.barrier()
         job_ms = bench.max_over_ranks(local_ms, dist, "cpu")
         job_channels = bench.sum_over_ranks(100 + rank, dist, "cpu")  # per-rank counts add up
-        # the config-4 and config-5 channel lists, each rank taking its share
+        # the ragged-batch and streaming channel lists, each rank taking its share
         import bench_workloads as W
         Es, TAs = W.config4_channels()
         costs4 = [bench.vis_ops(E, 4 * T, 1) for E, T in zip(Es, TAs)]

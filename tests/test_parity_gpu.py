@@ -1,7 +1,7 @@
 """GPU parity of libchimex against the CPU oracle, through the C ABI.
 
 Bit-exact integer comparisons: every output word must equal the oracle's.
-Small and golden cases compare whole buffers.  At the full BASELINE sizes one
+Small and golden cases compare whole buffers.  At the full benchmark sizes one
 channel per configuration is compared word for word with the oracle run on
 all host cores, and every channel is checked by size-independent properties:
 weighted checksums over every visibility (complex nonzero weights, four
@@ -238,7 +238,7 @@ def _config3():
 
 
 def _config3_single_channel():
-    """Config 3 with generate_frequency = 5: channel 5 random (seed 42, no
+    """The overflow workload with generate_frequency = 5: channel 5 random (seed 42, no
     repeat), every other channel the default value re = 7, im = -8
     (input_generator.c:84-96)."""
     if "c3q" not in _FULL:
@@ -250,7 +250,7 @@ def _config3_single_channel():
 
 @pytest.mark.parametrize("algo", ALGOS)
 def test_full_size_plain_config(chimex, algo):
-    """E=2048, F=8, T=16384, random no-repeat."""
+    """The full-size plain workload: E=2048, F=8, T=16384, random no-repeat."""
     E, F, T, packed, f, ref = _config2()
     blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
     np.testing.assert_array_equal(fc.channel_blocks(blocks, E, f), ref)
@@ -262,7 +262,7 @@ def test_full_size_plain_config(chimex, algo):
 
 @pytest.mark.parametrize("algo", ALGOS)
 def test_full_size_overflow_edge_config(chimex, algo):
-    """BASELINE config 3: constant -8 channels reach |Re| = 128 T exactly;
+    """The long-integration overflow workload: constant -8 channels reach |Re| = 128 T exactly;
     the random channels are checked word for word (one) and by checksums."""
     E, F, T, packed, f, ref = _config3()
     blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
@@ -278,7 +278,7 @@ def test_full_size_overflow_edge_config(chimex, algo):
 
 @pytest.mark.parametrize("algo", ALGOS)
 def test_full_size_single_channel_generator(chimex, algo):
-    """Config 3 with generate_frequency: the fixed channels hold exactly
+    """The overflow workload with generate_frequency: the fixed channels hold exactly
     T * |7 - 8i|^2 = 113 T (imaginary 0) in every cell, the generated channel
     equals the oracle word for word."""
     E, F, T, packed, q, ref = _config3_single_channel()
@@ -295,7 +295,7 @@ def test_full_size_single_channel_generator(chimex, algo):
 @pytest.mark.parametrize("ut", [0, 1])
 def test_full_size_offset_sums_and_preseed(chimex, kb, ut):
     """The standalone offset_accumulator and all four preseed variants at
-    config 3's size (E=2048, F=16, T=15296), word for word against the
+    the overflow workload's size (E=2048, F=16, T=15296), word for word against the
     oracle's restatement of offset_accumulator.cl:18-47 and
     preseed_multifreq*_UT.cl / preseed_multifreq*.cl."""
     E, F, T, packed, _, _ = _config3()

@@ -66,7 +66,7 @@ def test_stream_dumps_match_oracle(chimex):
 
 @pytest.mark.gpu
 def test_stream_config5_shape_dumps_match_oracle(chimex):
-    """Config 5's channel shape: E=2048 and E=1024 channels, time_accum 1024,
+    """The streaming workload's channel shape: E=2048 and E=1024 channels, time_accum 1024,
     frames of 256 samples, three integrations per channel with staggered
     starts (so completions of different channels fall on different ticks and
     on the same tick); every dump is compared word for word with the oracle
