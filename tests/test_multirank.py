@@ -104,3 +104,22 @@ def test_reference_arm_under_torchrun_prints_once():
     assert rec["n_gpus"] == 2
     assert rec["cpu_baseline"]["kind"] == "reference"
     assert rec["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_gpus_flag_relaunches_under_torchrun():
+    """`bench.py --gpus 2` started as a plain process relaunches itself as two
+    torchrun ranks (here on the reference arm, which needs no GPU): one JSON
+    line, from rank 0, reporting both ranks."""
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "cpu_corr_ref")
+    if not os.path.exists(ref_bin):
+        pytest.skip("reference CPU build absent")
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT")}
+    env.update(OMP_NUM_THREADS="1", MASTER_PORT=str(free_port()))
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--steps", "1", "--warmup", "3", "--ref-sample", "16"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    assert json.loads(lines[0])["n_gpus"] == 2
