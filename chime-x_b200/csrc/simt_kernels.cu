@@ -163,73 +163,83 @@ correlate_simt_kernel(const uint8_t *__restrict__ packed, int32_t *__restrict__ 
         }
 }
 
-// offsetAccumulateElements (offset_accumulator.cl:18-47).  A CTA owns 32
-// consecutive 16-byte vectors of a sample row (16 (f, e) bytes each) and a
-// sample range; warp w streams the range's 16-sample groups w, w + 8, ...
-// (each lane one vector: coalesced 512-byte rows), loading a group's 16
-// vectors at once so that enough bytes are in flight to keep HBM busy.  The
-// nibbles are summed four lanes at a time in byte-wide SWAR registers
-// (15 * 16 < 256) and flushed to 32-bit sums after every group; the 8 warps'
-// sums meet in shared memory, and the CTAs' in one atomic add per word.
+// offsetAccumulateElements (offset_accumulator.cl:18-47).  The work is the
+// (vector block, 16-sample group) space: a vector block is 32 consecutive
+// 16-byte vectors of a sample row (16 (f, e) bytes each), a group 16 samples.
+// Each CTA takes an equal, contiguous share of that space (so every SM of the
+// single wave streams the same number of bytes); inside a share, warp w
+// streams the groups w, w + 8, ... of one vector block at a time (each lane
+// one vector: coalesced 512-byte rows), loading a group's 16 vectors at once
+// so that enough bytes are in flight to keep HBM busy.  The nibbles are summed
+// four lanes at a time in byte-wide SWAR registers (15 * 16 < 256) and flushed
+// to 32-bit sums after every group; the 8 warps' sums meet in shared memory,
+// and the CTAs' in one atomic add per word for each vector block they touch.
 constexpr int kOaWarps = 8;
 
 __global__ void __launch_bounds__(kOaWarps * 32)
 offset_accumulate_kernel(const uint8_t *__restrict__ packed, uint32_t *__restrict__ sums,
-                         int64_t nvec, int T, int tchunk) {
+                         int64_t nvec, int T, int64_t ngroups, int64_t nwork) {
     __shared__ uint32_t part[kOaWarps][32][32];  // [warp][word][lane]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t i = (int64_t)blockIdx.x * 32 + lane;
-    const int t_begin = blockIdx.y * tchunk;
-    const int t_end = min(T, t_begin + tchunk);
     const uint4 *p = reinterpret_cast<const uint4 *>(packed);
-    uint32_t s[32];  // element 4q + j: s[2 (4q + j)] re, s[2 (4q + j) + 1] im
+    const int64_t L1 = nwork * (blockIdx.x + 1) / gridDim.x;
+    for (int64_t L = nwork * blockIdx.x / gridDim.x; L < L1;) {  // uniform across the CTA
+        const int64_t vb = L / ngroups;
+        const int64_t end = min(L1, (vb + 1) * ngroups);  // this vector block's part
+        const int64_t g0 = L - vb * ngroups, g1 = end - vb * ngroups;
+        const int64_t i = vb * 32 + lane;
+        uint32_t s[32];  // element 4q + j: s[2 (4q + j)] re, s[2 (4q + j) + 1] im
 #pragma unroll
-    for (int k = 0; k < 32; k++) s[k] = 0u;
-    if (i < nvec) {
-        for (int t = t_begin + 16 * w; t < t_end; t += 16 * kOaWarps) {
-            uint32_t lo[4] = {0u, 0u, 0u, 0u}, hi[4] = {0u, 0u, 0u, 0u};
-            const uint4 *row = p + (int64_t)t * nvec + i;
-            auto add = [&](const uint4 v) {
-                lo[0] += v.x & 0x0F0F0F0Fu;
-                hi[0] += (v.x >> 4) & 0x0F0F0F0Fu;
-                lo[1] += v.y & 0x0F0F0F0Fu;
-                hi[1] += (v.y >> 4) & 0x0F0F0F0Fu;
-                lo[2] += v.z & 0x0F0F0F0Fu;
-                hi[2] += (v.z >> 4) & 0x0F0F0F0Fu;
-                lo[3] += v.w & 0x0F0F0F0Fu;
-                hi[3] += (v.w >> 4) & 0x0F0F0F0Fu;
-            };
-            if (t + 16 <= t_end) {  // a full group: 16 independent loads in flight
-                uint4 v[16];
+        for (int k = 0; k < 32; k++) s[k] = 0u;
+        if (i < nvec) {
+            for (int64_t g = g0 + w; g < g1; g += kOaWarps) {
+                const int t = (int)(16 * g);
+                uint32_t lo[4] = {0u, 0u, 0u, 0u}, hi[4] = {0u, 0u, 0u, 0u};
+                const uint4 *row = p + (int64_t)t * nvec + i;
+                auto add = [&](const uint4 v) {
+                    lo[0] += v.x & 0x0F0F0F0Fu;
+                    hi[0] += (v.x >> 4) & 0x0F0F0F0Fu;
+                    lo[1] += v.y & 0x0F0F0F0Fu;
+                    hi[1] += (v.y >> 4) & 0x0F0F0F0Fu;
+                    lo[2] += v.z & 0x0F0F0F0Fu;
+                    hi[2] += (v.z >> 4) & 0x0F0F0F0Fu;
+                    lo[3] += v.w & 0x0F0F0F0Fu;
+                    hi[3] += (v.w >> 4) & 0x0F0F0F0Fu;
+                };
+                if (t + 16 <= T) {  // a full group: 16 independent loads in flight
+                    uint4 v[16];
 #pragma unroll
-                for (int k = 0; k < 16; k++) v[k] = __ldg(row + (int64_t)k * nvec);
+                    for (int k = 0; k < 16; k++) v[k] = __ldg(row + (int64_t)k * nvec);
 #pragma unroll
-                for (int k = 0; k < 16; k++) add(v[k]);
-            } else {
-                for (int k = 0; t + k < t_end; k++) add(__ldg(row + (int64_t)k * nvec));
-            }
+                    for (int k = 0; k < 16; k++) add(v[k]);
+                } else {
+                    for (int k = 0; t + k < T; k++) add(__ldg(row + (int64_t)k * nvec));
+                }
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+                for (int q = 0; q < 4; q++) {
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    s[2 * (4 * q + j)] += (hi[q] >> (8 * j)) & 0xFFu;
-                    s[2 * (4 * q + j) + 1] += (lo[q] >> (8 * j)) & 0xFFu;
+                    for (int j = 0; j < 4; j++) {
+                        s[2 * (4 * q + j)] += (hi[q] >> (8 * j)) & 0xFFu;
+                        s[2 * (4 * q + j) + 1] += (lo[q] >> (8 * j)) & 0xFFu;
+                    }
                 }
             }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < 32; k++) part[w][k][lane] = s[k];
-    __syncthreads();
-    // Thread r handles (word, lane) pairs r, r + 256, ...: sum over the warps.
+        for (int k = 0; k < 32; k++) part[w][k][lane] = s[k];
+        __syncthreads();
+        // Thread r handles (word, lane) pairs r, r + 256, ...: sum over the warps.
 #pragma unroll
-    for (int r = threadIdx.x; r < 32 * 32; r += kOaWarps * 32) {
-        const int k = r >> 5, l = r & 31;
-        const int64_t iv = (int64_t)blockIdx.x * 32 + l;
-        uint32_t acc = 0u;
+        for (int r = threadIdx.x; r < 32 * 32; r += kOaWarps * 32) {
+            const int k = r >> 5, l = r & 31;
+            const int64_t iv = vb * 32 + l;
+            uint32_t acc = 0u;
 #pragma unroll
-        for (int ww = 0; ww < kOaWarps; ww++) acc += part[ww][k][l];
-        if (iv < nvec && acc != 0u) atomicAdd(sums + 32 * iv + k, acc);
+            for (int ww = 0; ww < kOaWarps; ww++) acc += part[ww][k][l];
+            if (iv < nvec && acc != 0u) atomicAdd(sums + 32 * iv + k, acc);
+        }
+        __syncthreads();  // part is rewritten for the next vector block
+        L = end;
     }
 }
 
@@ -395,19 +405,16 @@ cudaError_t launch_offset_accumulate(const uint8_t *packed, uint32_t *sums, int 
                                      int T, cudaStream_t st) {
     const int64_t nvec = (int64_t)F * E / 16;  // E % 32 == 0
     const int64_t vblocks = (nvec + 31) / 32;
-    // One wave: three CTAs per SM fit (66 registers, 32 KiB shared memory),
-    // and a single wave beat two to four on B200 (4.66 vs 3.92 TB/s at E=2048,
-    // F=8, T=16384).  Sample ranges are a multiple of 8 warps x 16 samples,
-    // at most 65535 of them.
+    const int64_t ngroups = (T + 15) / 16;
+    const int64_t nwork = vblocks * ngroups;
+    // One wave of three CTAs per SM (66 registers, 32 KiB shared memory), each
+    // with an equal share of the work.
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int64_t chunks = std::max<int64_t>(1, (int64_t)3 * sms / std::max<int64_t>(1, vblocks));
-    chunks = std::min<int64_t>(chunks, (T + 127) / 128);
-    int tchunk = (int)(((T + chunks - 1) / chunks + 127) / 128 * 128);
-    while ((T + tchunk - 1) / tchunk > 65535) tchunk += 128;
-    dim3 grid((unsigned)vblocks, (unsigned)((T + tchunk - 1) / tchunk));
-    offset_accumulate_kernel<<<grid, kOaWarps * 32, 0, st>>>(packed, sums, nvec, T, tchunk);
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t)3 * sms, nwork));
+    offset_accumulate_kernel<<<(unsigned)grid, kOaWarps * 32, 0, st>>>(packed, sums, nvec, T,
+                                                                      ngroups, nwork);
     return cudaGetLastError();
 }
 
