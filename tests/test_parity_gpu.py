@@ -260,6 +260,17 @@ def test_full_size_plain_config(chimex, algo):
         fc.spot_checks(packed, blocks, T, F, E, g, rng, 16)
 
 
+def test_full_size_plain_config_nonstandard_convention(chimex):
+    """The full-size plain workload with upper_triangle_convention = 0 on the
+    SM-pair kernel: the same channel word for word (imaginary parts negated,
+    cpu_corr_test.c:91-96)."""
+    E, F, T, packed, f, ref = _config2()
+    blocks = gpu_blocks(chimex, packed, E, F, T, 0, "tc2")
+    want = ref.copy()
+    want[1::2] = (0 - want[1::2].astype(np.int64)).astype(np.int32)
+    np.testing.assert_array_equal(fc.channel_blocks(blocks, E, f), want)
+
+
 @pytest.mark.parametrize("algo", ALGOS)
 def test_full_size_overflow_edge_config(chimex, algo):
     """The long-integration overflow workload: constant -8 channels reach |Re| = 128 T exactly;

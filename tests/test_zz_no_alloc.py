@@ -146,3 +146,24 @@ def test_noalloc_check_reports_a_recorded_timeout_once():
     assert lib.chx_correlate_noalloc(_vp(packed), _vp(out), E, F, T, 1, 0, _stream()) == chimex.OK
     assert lib.chx_noalloc_check(_stream()) == chimex.OK
     np.testing.assert_array_equal(out.cpu().numpy(), orc.correlate_blocks(host, T, F, E, 1))
+
+
+@pytest.mark.gpu
+def test_noalloc_full_size_matches_plan_entry_point():
+    """The full-size plain workload (E=2048, F=8, T=16384: 288 SM-pair units)
+    through the allocation-free entry point, twice, against chx_correlate."""
+    _need_gpu()
+    import chimex
+    lib = chimex.lib()
+    E, F, T = 2048, 8, 16384
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(2048)
+    packed = torch.randint(0, 256, (T * F * E,), dtype=torch.uint8, device="cuda", generator=gen)
+    ref = chimex.Plan(E, F, T, 256, 1, 0, 0).correlate(packed)
+    out = torch.full_like(ref, -1)
+    for call in range(2):
+        rc = lib.chx_correlate_noalloc(_vp(packed), _vp(out), E, F, T, 1, 0, _stream())
+        assert rc == chimex.OK, lib.chx_last_error()
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref), "call %d" % call
+    assert lib.chx_noalloc_check(_stream()) == chimex.OK
