@@ -375,3 +375,25 @@ def test_tensor_core_path_rejects_unaligned_buffers(chimex):
     tri = torch.zeros(p.triangle_words + 8, dtype=torch.int32, device="cuda")
     assert lib.chx_blocks_to_triangle(h, ctypes.c_void_p(y.data_ptr()),
                                       ctypes.c_void_p(tri.data_ptr() + 8), s) == cx.E_INVALID
+
+
+@pytest.mark.parametrize("algo", ["tc", "tc2"])
+def test_large_element_count(chimex, algo):
+    """E=8192 (256 blocks per row, 32,896 blocks, 270 MB of output per channel)
+    on both tensor-core tiles, word for word against the oracle."""
+    E, F, T = 8192, 1, 96
+    packed = orc.generate(T, F, E, 4, 8192, no_repeat=1)
+    blocks = gpu_blocks(chimex, packed, E, F, T, 1, algo)
+    np.testing.assert_array_equal(blocks, orc.correlate_channel(packed, T, F, E, 0, 1))
+
+
+@pytest.mark.parametrize("algo", ["tc", "tc2"])
+def test_plan_above_the_unit_sample_limit(chimex, algo):
+    """T above 262144 samples: every tile pair is cut into ranges that meet by
+    TMA reduce-add, unsplit by the plan's own choice (tsplit 1) and split."""
+    E, F, T = 256, 2, 262144 + 100
+    packed = orc.generate(T, F, E, 4, 262, no_repeat=1)
+    ref = np.concatenate([orc.correlate_channel(packed, T, F, E, f, 1) for f in range(F)])
+    for tsplit in (1, 3):
+        np.testing.assert_array_equal(gpu_blocks(chimex, packed, E, F, T, 1, algo, tsplit=tsplit),
+                                      ref)
