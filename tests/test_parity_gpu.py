@@ -182,6 +182,44 @@ def test_reference_pipeline_compat(chimex, kb, ut, F, TA, algo):
     np.testing.assert_array_equal(full, orc.correlate_blocks(packed, T, F, E, ut))
 
 
+@pytest.mark.parametrize("E,F,T,tsplit", [(1920, 2, 2048, 0), (1408, 3, 1000, 3), (384, 4, 777, 2),
+                                          (1952, 1, 333, 0), (1888, 1, 500, 1)])
+def test_odd_tile_counts(chimex, E, F, T, tsplit):
+    """An odd number of 128-element tiles: the SM-pair kernel's last x pair
+    and last y pair hold one tile each (the missing tile's cells are computed
+    but never stored).  Every channel word for word against the oracle on
+    every kernel, then accumulated once more on the SM pair (E=1952 is an
+    even tile count with a partial last tile, E=1888 an odd one with a
+    partial last tile)."""
+    packed = orc.generate(T, F, E, 4, 5000 + E + T, no_repeat=1)
+    ref = np.concatenate([orc.correlate_channel(packed, T, F, E, f, 1) for f in range(F)])
+    for algo in ("tc2", "tc", "auto"):
+        np.testing.assert_array_equal(
+            gpu_blocks(chimex, packed, E, F, T, 1, algo, tsplit=tsplit), ref, err_msg=algo)
+    p = make_plan(chimex, E, F, T, algo="tc2", tsplit=tsplit)
+    d = to_dev(packed)
+    out = p.correlate(d)
+    p.correlate(d, out, accumulate=True)
+    p.check_device()
+    np.testing.assert_array_equal(out.cpu().numpy(), (ref.astype(np.int64) * 2).astype(np.int32))
+
+
+@pytest.mark.parametrize("kb,ut", [(0, 1), (0, 0), (1, 1)])
+def test_reference_pipeline_compat_odd_tiles(chimex, kb, ut):
+    """The reference corr partials (offset-nibble value maps) on the SM-pair
+    kernel with an odd tile count: E=384 (three tiles), F=1, TA=256."""
+    E, F, TA = 384, 1, 256
+    T = 2 * TA
+    packed = orc.generate(T, F, E, 4, 19, no_repeat=1)
+    p = make_plan(chimex, E, F, T, TA, ut, kb, "tc2")
+    d = to_dev(packed)
+    zero = torch.zeros(p.block_words, dtype=torch.int32, device="cuda")
+    np.testing.assert_array_equal(p.corr_compat(d, zero).cpu().numpy(),
+                                  orc.corr_partials(packed, T, F, E, kb, ut))
+    np.testing.assert_array_equal(p.reference_pipeline(d).cpu().numpy(),
+                                  orc.correlate_blocks(packed, T, F, E, ut))
+
+
 @pytest.mark.parametrize("kb,F,T,TA", [(0, 1, 592, 296), (0, 1, 100, 20), (0, 1, 120, 12),
                                          (1, 2, 512, 256), (1, 1, 4608, 2304)])
 def test_compat_rejects_outside_reference_domain(chimex, kb, F, T, TA):
