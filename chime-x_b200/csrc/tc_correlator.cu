@@ -34,9 +34,10 @@
 //              8-15 the x tile); then the epilogue (TMEM -> block layout).
 //   warp 16    TMA producer: packed y and x tiles, 32 samples per stage.
 //   warp 17    TMEM allocation and the single-thread MMA issue loop, which
-//              consumes stages in pairs (four Re MMAs, four Im MMAs, one
-//              commit) because switching accumulators or committing after
-//              every few MMAs stalls the tensor pipe.
+//              consumes stages in pairs (eight MMAs alternating between the
+//              Re and Im accumulators, one commit): committing after every
+//              few MMAs stalls the tensor pipe, and back-to-back MMAs into one
+//              accumulator wait for each other's TMEM update.
 // Every wait is bounded (globaltimer): on timeout the CTA records an error
 // code in the caller's error word, drains its MMAs and TMA loads and returns.
 #include "tc_common.cuh"
@@ -188,9 +189,9 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
         __syncwarp();
     } else if (warp == kMmaWarp) {
         // ------------------------------------------------------ MMA issuer
-        // Stages are consumed in pairs (64 samples): four Re MMAs, then four
-        // Im MMAs, then one commit releasing both operand slots.  Runs of
-        // MMAs into one accumulator and few commits keep the tensor pipe full.
+        // Stages are consumed in pairs (64 samples): eight MMAs alternating
+        // between the Re and Im accumulators, then one commit releasing both
+        // operand slots.
         if (lane == 0) {
             uint32_t gp = 0, acc_phase = 0;  // pair counter (pair gp uses slot gp & 1)
             bool ok = true;
@@ -222,18 +223,17 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                     }
                     tc_fence_after();
                     const uint32_t acc = (ip > 0) ? 1u : 0u;
+                    // Re and Im MMAs alternate: consecutive MMAs then go to
+                    // different accumulators and need not wait for each
+                    // other's TMEM update.
                     for (int j = 0; j < nin; j++) {
                         const int s = 2 * ps + j;
                         const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
                         const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
-                        mma_i8(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, (j > 0) ? 1u : acc);
+                        const uint32_t a0 = (j > 0) ? 1u : acc;
+                        mma_i8(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, a0);
+                        mma_i8(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, a0);
                         mma_i8(tmem_base, dRe1 + so_y, dX1 + so_x, idesc, 1u);
-                    }
-                    for (int j = 0; j < nin; j++) {
-                        const int s = 2 * ps + j;
-                        const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
-                        const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
-                        mma_i8(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, (j > 0) ? 1u : acc);
                         mma_i8(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);
                     }
                     mma_commit(empty_pair(ps));
