@@ -10,9 +10,9 @@
 // Each submit appends one frame per listed channel to its ring (in place when
 // the caller wrote it into the slot returned by chx_stream_frame_slot).  The
 // channels whose integration completes are correlated by one persistent
-// tensor-core launch over all their work units (two launches when channels of
-// both tile variants complete: the SM pair for an even 128-element tile count
-// or one of 15 and more, one SM for an odd count below 15): the integration's samples
+// tensor-core launch over all their work units (per tile variant: each
+// channel takes the plan path's default, the SM-pair kernel from E > 128 up
+// and the one-SM kernel below): the integration's samples
 // accumulate in TMEM and each dump buffer is written once, so the resident
 // state never travels through HBM per frame.  An event recorded after each
 // launch is waited for by the stream's completion thread, which records, per

@@ -476,20 +476,19 @@ cudaError_t launch_map(const TcLaunch &L, const CUtensorMap *pmap, const CUtenso
 
 }  // namespace
 
-// The SM-pair kernel's 256-element units cover an odd number nt of
-// 128-element tiles with a half-empty row and column of units: of its
-// (nt + 1) / 2 * ((nt + 1) / 2 + 1) / 2 units per channel, (nt + 1) / 2 do
-// half their tensor work or less in vain, 12 % of the work at nt = 15 and
-// more below.  The one-SM kernel wastes none but converts two x tiles per y
-// tile on one SM.  Measured on B200 with the automatic split (T = 16384,
-// TOPS, SM pair / one SM): every even tile count goes to the SM pair (E =
-// 256, F = 16: 1150 / 1040; 2048, F = 8: 2474 / 2133); odd counts from 15
-// tiles up as well (E = 1920, F = 8: 2182 / 2037; F = 16: 2182 / 2172); below
-// that the one-SM kernel (E = 1408, F = 8: 1834 / 2001; F = 16: 1873 / 2025;
-// E = 640: 918 / 1613).
+// The SM-pair kernel's 256-element units cover an odd number of 128-element
+// tiles with a half-empty row and column of units, whose missing tile's work
+// is done in vain; the one-SM kernel wastes none but converts two x tiles per
+// y tile on one SM.  Measured on B200 with the automatic split (T = 16384,
+// F = 8, TOPS, SM pair / one SM): E = 1920 2427 / 2024, 1664 1998 / 1775,
+// 1408 2051 / 1953, 1152 1903 / 1611, 896 1514 / 1473, 640 1418 / 1449,
+// 384 953 / 732, and 2048 2741 / 2133.  The SM pair is the default from two
+// tiles up; a single tile (E <= 128) would leave three quarters of its one
+// pair unit empty, so it goes to the one-SM kernel.  Both stay available as a
+// tile option and to the autotuner.
 int tc_default_tile(int E) {
     const int nt = (E + 127) / 128;
-    return (nt % 2 == 0 || nt >= 15) ? kTile2Sm : kTile1Sm;
+    return nt >= 2 ? kTile2Sm : kTile1Sm;
 }
 
 void tc_append_tile_units(int tile, std::vector<Unit> &out, int chan, int E, int t_begin,

