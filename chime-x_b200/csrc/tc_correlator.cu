@@ -18,14 +18,16 @@
 //
 // Shared-memory operands are MN-major (elements contiguous, like the input
 // bytes) with the 128-byte swizzle: an 8 k-row x 128-byte atom per 8 samples
-// and component.  One stage covers 32 samples:
-//   y: atoms [R0 I0 R1 I1 R2 I2 R3 I3 | I0 N0 I1 N1 I2 N2 I3 N3]   16 KiB
-//   x: per 128-element slice [X0 Y0 X1 Y1 X2 Y2 X3 Y3]             8 KiB per slice
-// (digit = 8-sample block; the I rows are stored twice so that every MMA
-// reads four consecutive atoms).  Four MMAs per stage (K = 32 each),
-// alternating accumulators so that consecutive MMAs are independent:
-//   Re += [R0 I0 R1 I1].[X0 Y0 X1 Y1]    Im += [I0 N0 I1 N1].[X0 Y0 X1 Y1]
-//   Re += [R2 I2 R3 I3].[X2 Y2 X3 Y3]    Im += [I2 N2 I3 N3].[X2 Y2 X3 Y3]
+// and component.  One stage covers 32 samples, each component's four atoms
+// contiguous (one MMA's K = 32 is one component over the stage's 32 samples):
+//   y: atoms [R0 R1 R2 R3 | I0 I1 I2 I3 | N0 N1 N2 N3]   12 KiB
+//   x: per 128-element slice [X0 X1 X2 X3 | Y0 Y1 Y2 Y3] 8 KiB per slice
+// (digit = 8-sample block).  Four MMAs per stage, alternating accumulators so
+// that consecutive MMAs are independent:
+//   Re += R.X    Im += I.X    Re += I.Y    Im += N.Y
+// Every operand row is stored once (a layout interleaving R and I per
+// 8-sample block needed the I rows twice: 16 KiB of y per stage, measured
+// 3-4 % slower on the SM-pair kernel, whose shared-memory traffic bounds it).
 //
 // Roles (576 threads, one persistent CTA per SM; each CTA works through its
 // own contiguous range of the unit table, assigned on the host by cost):
@@ -58,7 +60,7 @@ using namespace tc;
 constexpr int kStageSamples = kUnitStageSamples;
 constexpr int kOpStages = 4;    // operand ring
 constexpr int kPkStages = 6;    // packed-tile ring
-constexpr int kYOpBytes = 16 * 1024;
+constexpr int kYOpBytes = 16 * 1024;  // 12 KiB of operands; the slots also hold the epilogue staging
 constexpr int kXOpBytes = 16 * 1024;
 constexpr int kPkYBytes = kStageSamples * 128;      // 4 KiB
 constexpr int kPkXBytes = 2 * kPkYBytes;            // 8 KiB
@@ -196,10 +198,11 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
             uint32_t gp = 0, acc_phase = 0;  // pair counter (pair gp uses slot gp & 1)
             bool ok = true;
             const bool b_signed = (MAP == MAP_EXACT);
-            const uint64_t dRe0 = sdesc(op_y, 1024, 1024), dRe1 = sdesc(op_y + 4096, 1024, 1024);
-            const uint64_t dIm0 = sdesc(op_y + 8192, 1024, 1024);
-            const uint64_t dIm1 = sdesc(op_y + 12288, 1024, 1024);
-            const uint64_t dX0 = sdesc(op_x, 8192, 1024), dX1 = sdesc(op_x + 4096, 8192, 1024);
+            // per stage: y rows R, I, N and x rows X, Y (two 128-element
+            // slices 8 KiB apart), 32 samples each
+            const uint64_t dR = sdesc(op_y, 1024, 1024), dI = sdesc(op_y + 4096, 1024, 1024);
+            const uint64_t dN = sdesc(op_y + 8192, 1024, 1024);
+            const uint64_t dX = sdesc(op_x, 8192, 1024), dY = sdesc(op_x + 4096, 8192, 1024);
             for (int u = first; u < last && ok; u++) {
                 const Unit U = P.units[u];
                 const int nx = (U.tyx >> 20) & 3;
@@ -231,10 +234,10 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                         const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
                         const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
                         const uint32_t a0 = (j > 0) ? 1u : acc;
-                        mma_i8(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, a0);
-                        mma_i8(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, a0);
-                        mma_i8(tmem_base, dRe1 + so_y, dX1 + so_x, idesc, 1u);
-                        mma_i8(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);
+                        mma_i8(tmem_base, dR + so_y, dX + so_x, idesc, a0);        // Re += R X
+                        mma_i8(tmem_base + 256, dI + so_y, dX + so_x, idesc, a0);  // Im += I X
+                        mma_i8(tmem_base, dI + so_y, dY + so_x, idesc, 1u);        // Re += I Y
+                        mma_i8(tmem_base + 256, dN + so_y, dY + so_x, idesc, 1u);  // Im += N Y
                     }
                     mma_commit(empty_pair(ps));
                 }
@@ -267,7 +270,7 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
         const int sy = c >> 3, gy = c & 7;
         const uint32_t ry = (uint32_t)(sy & 7), by8 = (uint32_t)(sy >> 3);
         const uint32_t ldoff = (uint32_t)(sy * 128 + gy * 16);
-        const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);  // R (y) or X (x); I / Y at +1K
+        const uint32_t st_a = by8 * 1024 + swz(ry, gy);  // R (y) or X (x); I / Y at +4K, N at +8K
         uint32_t g = 0, gp_base = 0, acc_phase = 0, epi_phase = 0;
         bool ok = true;
         // Epilogue staging: 8 KiB per warp inside the operand slots, which
@@ -331,16 +334,15 @@ tc_correlate_kernel(const __grid_constant__ CUtensorMap pmap,
                 if (is_y) {
                     const uint32_t ya = op_y + os * kYOpBytes + st_a;
                     sts128(ya, v0[0], v0[1], v0[2], v0[3]);                // R
-                    sts128(ya + 1024, v1[0], v1[1], v1[2], v1[3]);         // I
-                    sts128(ya + 8192, v1[0], v1[1], v1[2], v1[3]);         // I (Im copy)
-                    sts128(ya + 8192 + 1024, v2[0], v2[1], v2[2], v2[3]);  // N
+                    sts128(ya + 4096, v1[0], v1[1], v1[2], v1[3]);  // I
+                    sts128(ya + 8192, v2[0], v2[1], v2[2], v2[3]);  // N
                 } else {
                     const uint32_t xa = op_x + os * kXOpBytes + st_a;
                     sts128(xa, v0[0], v0[1], v0[2], v0[3]);  // X slice 0
-                    sts128(xa + 1024, v1[0], v1[1], v1[2], v1[3]);  // Y slice 0
+                    sts128(xa + 4096, v1[0], v1[1], v1[2], v1[3]);  // Y slice 0
                     if (nx > 1) {
-                        sts128(xa + 8192, v2[0], v2[1], v2[2], v2[3]);  // X slice 1
-                        sts128(xa + 8192 + 1024, v3[0], v3[1], v3[2], v3[3]);  // Y slice 1
+                        sts128(xa + 8192, v2[0], v2[1], v2[2], v2[3]);         // X slice 1
+                        sts128(xa + 8192 + 4096, v3[0], v3[1], v3[2], v3[3]);  // Y slice 1
                     }
                 }
                 fence_proxy_async();

@@ -12,8 +12,8 @@
 //
 // Operand formulation, layout, value maps and the stage-pair MMA order are the
 // 1-SM kernel's (tc_correlator.cu); per CTA a 32-sample stage holds y
-// [R0 I0 R1 I1 R2 I2 R3 I3 | I0 N0 I1 N1 I2 N2 I3 N3] (16 KiB) and x
-// [X0 Y0 X1 Y1 X2 Y2 X3 Y3] (8 KiB).
+// [R0 R1 R2 R3 | I0 I1 I2 I3 | N0 N1 N2 N3] (12 KiB) and x
+// [X0 X1 X2 X3 | Y0 Y1 Y2 Y3] (8 KiB), each part an 8-sample atom.
 //
 // Warps: 0-15 unpack (0-7 y, 8-15 x), 16 TMA producer, 17 MMA issuer (CTA 0),
 // 18-25 epilogue.  The epilogue warps drain the accumulators of one unit while
@@ -48,7 +48,7 @@ constexpr int kStageSamples = kUnitStageSamples;
 constexpr int kOpSlots = 4;     // 2 stage pairs
 constexpr int kPairs = kOpSlots / 2;
 constexpr int kPkStages = 4;
-constexpr int kYOpBytes = 16 * 1024;
+constexpr int kYOpBytes = 12 * 1024;
 constexpr int kXOpBytes = 8 * 1024;
 constexpr int kPkBytes = kStageSamples * 128;  // one 128-element tile, 4 KiB
 constexpr int kUnpackWarps = 16;
@@ -189,11 +189,11 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                 const uint32_t idesc = (2u << 4) | (1u << 7) | ((b_signed ? 1u : 0u) << 10) |
                                        (1u << 15) | (1u << 16) | ((256u >> 3) << 17) |
                                        ((256u >> 4) << 24);
-                const uint64_t dRe0 = sdesc(op_y, 1024, 1024);
-                const uint64_t dRe1 = sdesc(op_y + 4096, 1024, 1024);
-                const uint64_t dIm0 = sdesc(op_y + 8192, 1024, 1024);
-                const uint64_t dIm1 = sdesc(op_y + 12288, 1024, 1024);
-                const uint64_t dX0 = sdesc(op_x, 1024, 1024), dX1 = sdesc(op_x + 4096, 1024, 1024);
+                // per stage: y rows R, I, N and x rows X, Y, 32 samples each
+                const uint64_t dR = sdesc(op_y, 1024, 1024);
+                const uint64_t dI = sdesc(op_y + 4096, 1024, 1024);
+                const uint64_t dN = sdesc(op_y + 8192, 1024, 1024);
+                const uint64_t dX = sdesc(op_x, 1024, 1024), dY = sdesc(op_x + 4096, 1024, 1024);
                 for (int u = first; u < last && ok; u++) {
                     const Unit U = P.units[u];
                     const int nst = (U.t1 - U.t0 + kStageSamples - 1) / kStageSamples;
@@ -222,10 +222,10 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                             const uint64_t so_y = (uint64_t)((s * kYOpBytes) >> 4);
                             const uint64_t so_x = (uint64_t)((s * kXOpBytes) >> 4);
                             const uint32_t a0 = (j > 0) ? 1u : acc;
-                            mma_i8_pair(tmem_base, dRe0 + so_y, dX0 + so_x, idesc, a0);
-                            mma_i8_pair(tmem_base + 256, dIm0 + so_y, dX0 + so_x, idesc, a0);
-                            mma_i8_pair(tmem_base, dRe1 + so_y, dX1 + so_x, idesc, 1u);
-                            mma_i8_pair(tmem_base + 256, dIm1 + so_y, dX1 + so_x, idesc, 1u);
+                            mma_i8_pair(tmem_base, dR + so_y, dX + so_x, idesc, a0);        // Re += R X
+                            mma_i8_pair(tmem_base + 256, dI + so_y, dX + so_x, idesc, a0);  // Im += I X
+                            mma_i8_pair(tmem_base, dI + so_y, dY + so_x, idesc, 1u);        // Re += I Y
+                            mma_i8_pair(tmem_base + 256, dN + so_y, dY + so_x, idesc, 1u);  // Im += N Y
                         }
                         mma_commit_pair(bar(kBarEmptyPair + ps));
                     }
@@ -253,7 +253,7 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
         const int sy = c >> 3, gy = c & 7;
         const uint32_t ry = (uint32_t)(sy & 7), by8 = (uint32_t)(sy >> 3);
         const uint32_t ldoff = (uint32_t)(sy * 128 + gy * 16);
-        const uint32_t st_a = (2 * by8) * 1024 + swz(ry, gy);
+        const uint32_t st_a = by8 * 1024 + swz(ry, gy);  // R or X; I / Y at +4K, N at +8K
         const uint32_t full_pair_leader = mapa(bar(kBarFullPair), 0);
         uint32_t g = 0, gp = 0;
         bool ok = true;
@@ -316,13 +316,12 @@ tc_pair_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__
                     if (is_y) {
                         const uint32_t ya = op_y + os * kYOpBytes + st_a;
                         sts128(ya, v0[j][0], v0[j][1], v0[j][2], v0[j][3]);                // R
-                        sts128(ya + 1024, v1[j][0], v1[j][1], v1[j][2], v1[j][3]);         // I
-                        sts128(ya + 8192, v1[j][0], v1[j][1], v1[j][2], v1[j][3]);         // I
-                        sts128(ya + 8192 + 1024, v2[j][0], v2[j][1], v2[j][2], v2[j][3]);  // N
+                        sts128(ya + 4096, v1[j][0], v1[j][1], v1[j][2], v1[j][3]);  // I
+                        sts128(ya + 8192, v2[j][0], v2[j][1], v2[j][2], v2[j][3]);  // N
                     } else {
                         const uint32_t xa = op_x + os * kXOpBytes + st_a;
                         sts128(xa, v0[j][0], v0[j][1], v0[j][2], v0[j][3]);         // X
-                        sts128(xa + 1024, v1[j][0], v1[j][1], v1[j][2], v1[j][3]);  // Y
+                        sts128(xa + 4096, v1[j][0], v1[j][1], v1[j][2], v1[j][3]);  // Y
                     }
                 }
                 fence_proxy_async();
